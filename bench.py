@@ -1,0 +1,342 @@
+"""Benchmark: PMCHWT MLFMA matvecs/s on one B200 (plain FP64 path).
+
+Workload (default): dielectric sphere of radius 5 lambda at 300 MHz,
+icosphere subdivided 6 times (81,920 triangles, 122,880 RWGs, 245,760
+unknowns), eps_r = 2.5 - 0.1j, leaf box 0.25 lambda, 7-point rule; x seeded
+uniform on the unit disk (mt19937_64 seed 0). Synthetic mesh (the
+reference's meshes are not distributed). A step is one operator application
+w = A x. The operator tables (8.7 GB of leaf patterns alone) are far larger
+than L2, so no explicit flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints ONE JSON line on rank 0. Under torchrun every rank runs an
+independent replica on its own GPU (the path does not shard: "replicas
+only"); the device time is the max over ranks and value = total matvecs of
+all ranks / that time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PMCHWT solve s/RHS to 1e-3 residual & matvec/s vs plain FP64 GPU MLFMA path"
+UNIT = "matvec/s"
+FREQ = 3.0e8
+
+
+def workload(args):
+    from mlfma_pmchwt_b200 import mesh as M
+    lam = M.wavelength(FREQ)
+    if args.size == "full":
+        return dict(name="sphere r=5 lambda, icosphere sub 6, 245,760 unknowns, eps_r 2.5-0.1j, leaf 0.25 lambda, "
+                         "7-pt rule, FP64", sub=6, radius=5 * lam, eps=complex(2.5, -0.1), leaf=0.25)
+    return dict(name="sphere r=1 m, icosphere sub 3, 3,840 unknowns, eps_r 4, leaf 0.25 lambda, 7-pt rule, FP64",
+                sub=3, radius=1.0, eps=complex(4.0, 0.0), leaf=0.25)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self._t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [q.strip() for q in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def allreduce_max(v: float, world: int, device) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def stage_bytes(op) -> dict:
+    """Algorithmic bytes per apply for each stage, every operand touched once."""
+    inf = op.info
+    L = op.max_level
+    c16 = 16.0
+    b = {"aggregation": 0.0, "interpolation_up": 0.0, "translation_down": 0.0, "leaf_testing_near": 0.0}
+    for Ks in (inf.K_k1, inf.K_k2):
+        Kl = Ks[L - 2]
+        Bl = inf.boxes[L - 2]
+        b["aggregation"] += op.N * 3 * Kl * c16 + Bl * 6 * Kl * c16
+        for l in range(2, L):
+            i = l - 2
+            b["interpolation_up"] += inf.boxes[i + 1] * 6 * Ks[i + 1] * c16 + inf.boxes[i] * 6 * Ks[i] * c16
+        for l in range(2, L + 1):
+            i = l - 2
+            nvec = 316  # upper bound of the translation table rows at a level
+            b["translation_down"] += 2 * inf.boxes[i] * 6 * Ks[i] * c16 + min(nvec, 343) * Ks[i] * c16 * 0
+            if l > 2:
+                b["translation_down"] += inf.boxes[i - 1] * 6 * Ks[i - 1] * c16
+        b["leaf_testing_near"] += op.N * 3 * Kl * c16 + Bl * 6 * Kl * c16
+    b["leaf_testing_near"] += inf.near_pairs * 3 * c16 + 4 * op.n * c16
+    return b
+
+
+def cpu_baseline_reference(args, wl, rank: int) -> dict | None:
+    """The reference's own OpenMP matvec (oracle/_ref) on this host's cores."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    from mlfma_pmchwt_b200 import mesh as M
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    m = M.icosphere(wl["sub"], wl["radius"])
+    nas = M.write_nas(m, Path("/tmp") / f"bench_ref_{os.getpid()}.nas")
+    t0 = time.perf_counter()
+    ref = O.RefOperator(nas, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"])
+    setup = time.perf_counter() - t0
+    x = M.unit_disk_vector(ref.n, 0)
+    ref.apply(x)  # warm-up
+    times = []
+    budget = args.cpu_budget
+    t_start = time.perf_counter()
+    while True:
+        t = time.perf_counter()
+        ref.apply(x)
+        times.append(time.perf_counter() - t)
+        if time.perf_counter() - t_start > budget or len(times) >= 50:
+            break
+    ref.close()
+    return {"value": 1.0 / float(np.median(times)), "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{len(times)} full reference matvecs (median) of the same operator after its "
+                      f"{setup:.1f} s OpenMP setup; oracle/_ref built from the reference sources",
+            "setup_s": setup}
+
+
+def run_reference_arm(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    wl = workload(args)
+    base = cpu_baseline_reference(args, wl, rank)
+    if base is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmlfma_ref.so not built"}))
+        return 0
+    # steps: each step one reference matvec (bounded by --cpu-budget)
+    line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / base["value"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": wl["name"], "parallelism": "openmp", "l2": "inputs larger than L2"},
+            "impl": "reference", "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_product(args):
+    import torch
+    from mlfma_pmchwt_b200 import MLFMM
+    from mlfma_pmchwt_b200 import mesh as M
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    wl = workload(args)
+    m = M.icosphere(wl["sub"], wl["radius"])
+    t0 = time.perf_counter()
+    op = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local)
+    setup_s = time.perf_counter() - t0
+    n = op.n
+    x_host = M.unit_disk_vector(n, 0)
+    x = torch.from_numpy(x_host).to(dev)
+    w = torch.empty(n, dtype=torch.complex128, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step():
+        op.apply_device(x.data_ptr(), w.data_ptr(), sp)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    # timed region: device time, max over ranks
+    op.profile(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    ms_local = e0.elapsed_time(e1)
+    stage_ms, napp = op.stage_times()
+    op.profile(False)
+    ms_total = allreduce_max(ms_local, world, dev)
+    ms_per_step = ms_total / args.steps
+    value = world * args.steps / (ms_total / 1000.0)
+
+    # end to end through the C ABI with pinned host buffers
+    xh = torch.from_numpy(x_host).pin_memory()
+    wh = torch.empty(n, dtype=torch.complex128).pin_memory()
+    xh_np, wh_np = xh.numpy(), wh.numpy()
+    for _ in range(2):
+        op._lib.mlfma_apply(op._h, n, xh_np.ctypes.data_as(_dp_t()), wh_np.ctypes.data_as(_dp_t()))
+    barrier(world)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        rc = op._lib.mlfma_apply(op._h, n, xh_np.ctypes.data_as(_dp_t()), wh_np.ctypes.data_as(_dp_t()))
+        if rc != 0:
+            raise RuntimeError(op._lib.mlfma_last_error().decode())
+    e2e_s = allreduce_max(time.perf_counter() - t, world, dev)
+    barrier(world)
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * 16,
+           "d2h_bytes_per_step": n * 16}
+
+    # roofline of the dominant stage (HBM-bound FP64 path)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    sb = stage_bytes(op)
+    per_apply_ms = {k: v / max(napp, 1) for k, v in stage_ms.items()}
+    dom = max(per_apply_ms, key=per_apply_ms.get)
+    achieved = sb[dom] / (per_apply_ms[dom] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": None,
+                "algorithmic_bytes": sb[dom],
+                "stage_ms_per_apply": {k: round(v, 4) for k, v in per_apply_ms.items()},
+                "matvec_bytes": sum(sb.values()),
+                "matvec_frac": round(sum(sb.values()) / (ms_per_step / 1000.0) / 1e9 / peak, 4)}
+
+    # one GMRES(50) solve of the plane-wave excitation, capped iterations
+    solve = None
+    if args.solve_its > 0:
+        from mlfma_pmchwt_b200 import plane_wave
+        V = op.compute_v_pmchwt(*plane_wave(0.0, 0.0, 0.0))
+        xs, st = op.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3)
+        solve = {"s_per_rhs": round(st["seconds"], 4), "iterations": st["iterations"], "converged": st["converged"],
+                 "rel_residual": st["rel_residual"], "restart": 50, "tol": 1e-3, "itr_max": args.solve_its}
+
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": wl["name"], "unknowns": n, "max_level": op.max_level,
+                       "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
+                       "setup_s": round(setup_s, 2), "device_bytes": op.info.bytes_device},
+            "e2e": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in e2e.items()},
+            "gpu_launches": args.steps * (2 * (1 + 2 * (op.max_level - 2) + 1) + 1),
+            "roofline": roofline, "clocks": clk}
+    if solve:
+        line["solve"] = solve
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline_reference(args, wl, rank)
+        if base:
+            line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line))
+    op.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def _dp_t():
+    import ctypes
+    return ctypes.POINTER(ctypes.c_double)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["product", "reference"], default="product")
+    ap.add_argument("--size", choices=["full", "small"], default="full")
+    ap.add_argument("--solve-its", type=int, default=300)
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference matvecs to time")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_product(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

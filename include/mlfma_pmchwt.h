@@ -1,0 +1,219 @@
+/*
+ * mlfma_pmchwt.h -- C ABI of the B200 PMCHWT MLFMA operator and Krylov solve.
+ *
+ * This is the drop-in boundary for the dielectric (PMCHWT) MLFMA path of the
+ * reference solver CCCCl0uD/MLFMA_PMCHWT. Every entry point names the
+ * reference interface it replaces (path:line inside the reference project).
+ *
+ * Conventions
+ *  - Complex vectors are interleaved float64 pairs (re, im), the memory layout
+ *    of std::complex<double> and of C99 double _Complex.
+ *  - Unknown ordering is the reference's: n = 2N for N RWG functions;
+ *    x[0:N) = J coefficients, x[N:2N) = M coefficients (Code/MLFMM.cpp:239-245).
+ *    RWG order is the reference's RWG numbering (Code/RWGGenerator.cpp:41-72:
+ *    common edges in ascending (min vertex id, max vertex id) order).
+ *  - No C++ exception crosses this boundary. Every function returns an int
+ *    status: MLFMA_OK (0) or a negative code; mlfma_last_error() gives the
+ *    message of the last failure on the calling thread.
+ *  - One apply/solve in flight per plan (the plan owns its work arrays, as the
+ *    reference's MLFMM object owns Sm/Bm, Code/MLFMM.h:60-66). Different plans
+ *    may run concurrently.
+ */
+#ifndef MLFMA_PMCHWT_H
+#define MLFMA_PMCHWT_H
+
+#if defined(__GNUC__)
+#define MLFMA_API __attribute__((visibility("default")))
+#else
+#define MLFMA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MLFMA_OK 0
+#define MLFMA_ERR_ARG (-1)        /* bad argument: null pointer, size mismatch, n <= 0 */
+#define MLFMA_ERR_MESH (-2)       /* mesh / NAS input unusable */
+#define MLFMA_ERR_CUDA (-3)       /* CUDA runtime error */
+#define MLFMA_ERR_NOMEM (-4)      /* device or host allocation failed */
+#define MLFMA_ERR_UNSUPPORTED (-5)/* option not supported */
+#define MLFMA_ERR_NOT_CONVERGED 1 /* solve ended without meeting the tolerance (not an error) */
+
+typedef struct mlfma_plan mlfma_plan;
+
+/* Triangle mesh in NAS terms (Code/NASReader.cpp:60-144): GRID ids with
+ * coordinates, CTRIA3 ids with three GRID ids each. Faces keep file order. */
+typedef struct {
+  int num_points;
+  const int* point_ids;        /* [num_points] GRID ids */
+  const double* xyz;           /* [3*num_points] */
+  int num_faces;
+  const int* face_ids;         /* [num_faces] CTRIA3 ids */
+  const int* face_points;      /* [3*num_faces] GRID ids of vertex1..3 */
+} mlfma_mesh;
+
+/* Physical and discretisation parameters. Defaults (mlfma_default_params):
+ * the reference's EMSource / PhyConstant / main.cpp values. */
+typedef struct {
+  double freq_hz;              /* EMSource(freq), Code/EMSource.cpp:6-14 */
+  double eps_r_re, eps_r_im;   /* EMSource::initDielectric, Code/EMSource.cpp:19-32 */
+  double mu_r_re, mu_r_im;
+  double leaf_coeff;           /* leaf box edge in wavelengths (Code/PhyConstant.h:14; 0.3) */
+  int gauss_points;            /* triangle rule: 1,3,4,6,7,12,13,16 (Code/GaussPoints.cpp:286-299) */
+  int precision;               /* MLFMA_PREC_FP64 */
+  int device;                  /* CUDA device ordinal */
+  int verbose;                 /* print setup summary to stderr */
+} mlfma_params;
+
+#define MLFMA_PREC_FP64 0
+
+typedef struct {
+  int num_rwg;                 /* N */
+  int num_unknowns;            /* 2N */
+  int max_level;               /* OCTree::maxLevel_ */
+  int num_levels;              /* MLFMA levels 2..max_level */
+  int boxes[16];               /* boxes at level 2+i */
+  int L_k1[16], L_k2[16];      /* multipole order at level 2+i */
+  int K_k1[16], K_k2[16];      /* directions at level 2+i */
+  long long near_pairs;        /* RWG pairs in the near field */
+  long long far_pairs[16];     /* interaction-list pairs at level 2+i */
+  double bytes_device;         /* device bytes held by the plan */
+  double setup_seconds;        /* wall time of mlfma_plan_create */
+  double k1_re, k1_im, k2_re, k2_im, etai_re, etai_im, wavelength;
+} mlfma_info;
+
+typedef struct {
+  int iterations;              /* inner Arnoldi steps taken (MGMRES total_iter) */
+  int restarts;                /* restart cycles */
+  int matvecs;                 /* operator applications */
+  int converged;               /* 1 if the tolerance was met */
+  double rel_residual;         /* last true residual ||b - A x|| / ||b|| */
+  double seconds;              /* device time of the solve */
+  int history_len;             /* entries written to history */
+} mlfma_solve_stats;
+
+MLFMA_API void mlfma_default_params(mlfma_params* p);
+MLFMA_API const char* mlfma_last_error(void);
+MLFMA_API const char* mlfma_version(void);
+
+/* Builds the operator: RWGs (Code/RWGGenerator.cpp:39-113), octree
+ * (Code/OCTree.cpp:13-32), angular grids (Code/AlgoMLFMM.h:21-138),
+ * transfer factors (:192-295), interpolation (:298-368), radiation/receive
+ * patterns (Code/ProcessFMM.h:217-233) and the near-field PMCHWT rows
+ * (Code/Zmartix.h:541-643) -- replaces the setup half of the MLFMM
+ * constructor (Code/MLFMM.cpp:15-113). Patterns, transfer factors and the
+ * near field are computed on the GPU. */
+MLFMA_API int mlfma_plan_create(const mlfma_mesh* mesh, const mlfma_params* params, mlfma_plan** plan);
+
+/* Same, reading a NAS file in the dialect of Code/NASReader.cpp:60-144. */
+MLFMA_API int mlfma_plan_create_nas(const char* nas_path, const mlfma_params* params, mlfma_plan** plan);
+
+MLFMA_API int mlfma_plan_destroy(mlfma_plan* plan);
+MLFMA_API int mlfma_plan_info(const mlfma_plan* plan, mlfma_info* info);
+
+/* w = A x, the PMCHWT MLFMA matvec: the `ax` closure of
+ * MLFMM::matrix_solver (Code/MLFMM.cpp:189-368), i.e. the documented
+ * MLFMM::applyAx(int n, const std::complex<double>* x, std::complex<double>* w).
+ * Host pointers; n must be 2N. w is overwritten. */
+MLFMA_API int mlfma_apply(mlfma_plan* plan, int n, const double* x, double* w);
+
+/* The same on device-resident vectors (complex128 [n]) on a CUDA stream
+ * (cudaStream_t passed as void*; NULL = the plan's stream). Asynchronous. */
+MLFMA_API int mlfma_apply_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream);
+
+/* Stage timing (no counterpart in the reference, whose timers are
+ * std::chrono prints): with on != 0 every apply records CUDA events on its
+ * stream between stage groups; mlfma_profile_read sums them since the last
+ * read into stage_ms[4] = {aggregation, interpolation up, translation +
+ * anterpolation down, leaf testing + near field} and the number of applies. */
+MLFMA_API int mlfma_profile(mlfma_plan* plan, int on);
+MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applies);
+
+/* Restarted GMRES(mr) with the operator -- replaces MGMRES::mgmres
+ * (Code/GMRES.h:65-217) driven by MLFMM::matrix_solver (Code/MLFMM.cpp:186).
+ * Same arguments and stopping rule: stop when ||r||/||b|| < tol_rel or
+ * < tol_abs, or after itr_max inner steps; true residual after each cycle;
+ * divergence abort after cycle 8. x holds the initial guess on entry and the
+ * solution on return (host pointers). history (optional, may be NULL) receives
+ * the estimated relative residual of each inner step, up to history_cap.
+ * Returns MLFMA_OK when converged, MLFMA_ERR_NOT_CONVERGED otherwise. */
+MLFMA_API int mlfma_gmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr,
+                double tol_abs, double tol_rel, mlfma_solve_stats* stats, double* history,
+                int history_cap);
+
+/* Plane-wave excitation vector V (complex128 [2N]) -- RHS::computeV_PMCHWT
+ * (Code/Vm.h:150-203) with the incident unit vectors of EMSource::initPW
+ * (Code/EMSource.cpp:34-72): kinc (propagation), einc (E polarisation),
+ * hinc (kinc x einc). Host pointers. */
+MLFMA_API int mlfma_rhs_pmchwt(mlfma_plan* plan, const double kinc[3], const double einc[3],
+                     const double hinc[3], double* V);
+
+/* Far-field of currents I (complex128 [2N]) at n_angles directions
+ * (degrees) -- RCSUtils::calculateRCS_PMCHWT (Code/RCS.h:116-192).
+ * field (optional): 3 complex Cartesian components per angle (6 doubles).
+ * rcs_db (optional): total / theta-pol / phi-pol RCS in dBsm per angle
+ * (3 doubles), formed as the dual-static study does (Code/RCS.h:391-410). */
+MLFMA_API int mlfma_rcs_pmchwt(mlfma_plan* plan, const double* I, int n_angles, const double* theta_deg,
+                     const double* phi_deg, double* field, double* rcs_db);
+
+/* Copies of the plan's tables, for verification against the reference.
+ * mlfma_get_rwgs: per RWG (reference order): face ids of T+ / T-, GRID ids of
+ * the free vertices and of the common edge, edge length, edge midpoint
+ * (RWGBase, Code/MyStruct.h:93-103). Any pointer may be NULL. */
+MLFMA_API int mlfma_get_rwgs(const mlfma_plan* plan, int* face_pos, int* face_neg, int* free_pos,
+                   int* free_neg, int* edge_a, int* edge_b, double* length, double* mid);
+
+/* Boxes of one octree level (physical level 2..max_level) in the plan's
+ * order (ascending Morton code): Morton codes and centres. Returns the count
+ * when the pointers are NULL. */
+MLFMA_API long long mlfma_get_level(const mlfma_plan* plan, int level, unsigned long long* morton,
+                          double* center);
+
+/* Stage arrays after the last apply, for stage-level comparison:
+ * which 0 = aggregated pattern Sm, 1 = incoming pattern Bm; medium 1 or 2;
+ * level = physical level; out: [boxes][6][K] complex (J xyz then M xyz).
+ * Returns the number of complex values (or that count when out is NULL). */
+MLFMA_API long long mlfma_get_stage(mlfma_plan* plan, int which, int medium, int level, double* out);
+
+/* Leaf radiation (which 0) / receive (which 1) patterns of medium 1|2 in
+ * reference RWG order: [N][K][3] complex (the layout of Vsmi/Vfmj). */
+MLFMA_API long long mlfma_get_pattern(mlfma_plan* plan, int medium, int which, double* out);
+
+/* Transfer factors of medium at a level as [vec][K] complex with the
+ * integer translation offsets (target - source, in box edges) [vec][3]. */
+MLFMA_API long long mlfma_get_transfer(mlfma_plan* plan, int medium, int level, int* offsets, double* tf);
+
+/* Near-field entries: per near RWG pair (target t, source s), in the plan's
+ * order: t, s (reference RWG ids) and z11, z12, z22 (Code/Zmartix.h:611-628;
+ * z21 = -z12). Returns the pair count when pointers are NULL. */
+MLFMA_API long long mlfma_get_near(mlfma_plan* plan, int* target, int* source, double* z11, double* z12,
+                         double* z22);
+
+/* Near (26-neighbourhood, Code/OCTree.cpp:385-426) and interaction lists
+ * (Code/OCTree.cpp:428-488) of a level in CSR form over the plan's box
+ * order; far_off is the encoded offset target - source,
+ * (dx+3)*49 + (dy+3)*7 + (dz+3). Returns the interaction-pair count. */
+MLFMA_API long long mlfma_get_level_lists(const mlfma_plan* plan, int level, int* near_ptr, int* near_idx,
+                                          int* far_ptr, int* far_idx, int* far_off);
+
+/* RWG ids of each leaf box (CSR): leaf_ptr [boxes+1], leaf_rwg [N]. Returns the box count. */
+MLFMA_API long long mlfma_get_leaf_rwgs(const mlfma_plan* plan, int* leaf_ptr, int* leaf_rwg);
+
+/* Angular grid of medium 1|2 at a physical level (Code/AlgoMLFMM.h:21-138):
+ * theta [L], phi [2L], Gauss-Legendre weights [L], phi weight. Returns L. */
+MLFMA_API int mlfma_get_grid(const mlfma_plan* plan, int medium, int level, double* theta, double* phi,
+                             double* wtheta, double* wphi);
+
+/* Interpolation from level+1 onto level (Code/AlgoMLFMM.h:298-368), in
+ * separable form: per parent theta row, three child theta indices and
+ * Lagrange weights; per parent phi column, three child phi indices and
+ * weights (the reference's 9 weights are the products lt * lp). */
+MLFMA_API int mlfma_get_interp(const mlfma_plan* plan, int medium, int level, int* tidx, double* lt, int* pidx,
+                               double* lp);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MLFMA_PMCHWT_H */

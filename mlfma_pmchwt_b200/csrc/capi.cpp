@@ -1,0 +1,442 @@
+// extern "C" boundary (include/mlfma_pmchwt.h). No exception crosses it:
+// every entry point maps failures onto status codes and records the message
+// for mlfma_last_error() on the calling thread.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+#include "../../include/mlfma_pmchwt.h"
+#include "plan.hpp"
+#include "solver.hpp"
+
+struct mlfma_plan {
+  std::unique_ptr<mlfma::Plan> p;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const mlfma::CudaError& e) {
+    return fail(MLFMA_ERR_CUDA, e.what());
+  } catch (const std::bad_alloc& e) {
+    return fail(MLFMA_ERR_NOMEM, "host allocation failed");
+  } catch (const std::invalid_argument& e) {
+    return fail(MLFMA_ERR_ARG, e.what());
+  } catch (const std::domain_error& e) {
+    return fail(MLFMA_ERR_MESH, e.what());
+  } catch (const std::exception& e) {
+    const std::string w = e.what();
+    if (w.find("cudaMalloc") != std::string::npos) return fail(MLFMA_ERR_NOMEM, w);
+    return fail(MLFMA_ERR_CUDA, w);
+  }
+}
+
+mlfma::PlanParams to_params(const mlfma_params* p) {
+  mlfma::PlanParams q;
+  q.freq = p->freq_hz;
+  q.epsr = mlfma::cplx(p->eps_r_re, p->eps_r_im);
+  q.mur = mlfma::cplx(p->mu_r_re, p->mu_r_im);
+  q.leaf_coeff = p->leaf_coeff;
+  q.gauss = p->gauss_points;
+  q.device = p->device;
+  q.verbose = p->verbose;
+  return q;
+}
+
+bool device_plan(const mlfma_plan* plan) { return plan && plan->p && plan->p->device >= 0; }
+
+}  // namespace
+
+extern "C" {
+
+void mlfma_default_params(mlfma_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->freq_hz = 3.0e8;
+  p->eps_r_re = 1.0;
+  p->mu_r_re = 1.0;
+  p->leaf_coeff = 0.3;
+  p->gauss_points = 7;
+  p->precision = MLFMA_PREC_FP64;
+  p->device = 0;
+}
+
+const char* mlfma_last_error(void) { return g_last_error.c_str(); }
+
+const char* mlfma_version(void) { return "mlfma_pmchwt_b200 0.1 (sm_100a, FP64)"; }
+
+int mlfma_plan_create(const mlfma_mesh* mesh, const mlfma_params* params, mlfma_plan** plan) {
+  if (!mesh || !params || !plan) return fail(MLFMA_ERR_ARG, "null argument");
+  *plan = nullptr;
+  return guarded([&] {
+    if (params->precision != MLFMA_PREC_FP64) return fail(MLFMA_ERR_UNSUPPORTED, "precision");
+    mlfma::Mesh m;
+    std::string err;
+    if (!mlfma::mesh_from_arrays(mesh->num_points, mesh->point_ids, mesh->xyz, mesh->num_faces, mesh->face_ids,
+                                 mesh->face_points, m, err))
+      return fail(MLFMA_ERR_MESH, err);
+    auto p = mlfma::create_plan(std::move(m), to_params(params));
+    *plan = new mlfma_plan{std::move(p)};
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_plan_create_nas(const char* nas_path, const mlfma_params* params, mlfma_plan** plan) {
+  if (!nas_path || !params || !plan) return fail(MLFMA_ERR_ARG, "null argument");
+  *plan = nullptr;
+  return guarded([&] {
+    if (params->precision != MLFMA_PREC_FP64) return fail(MLFMA_ERR_UNSUPPORTED, "precision");
+    mlfma::Mesh m;
+    std::string err;
+    if (!mlfma::read_nas(nas_path, m, err)) return fail(MLFMA_ERR_MESH, err);
+    auto p = mlfma::create_plan(std::move(m), to_params(params));
+    *plan = new mlfma_plan{std::move(p)};
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_plan_destroy(mlfma_plan* plan) {
+  if (!plan) return MLFMA_OK;
+  return guarded([&] {
+    delete plan;
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_plan_info(const mlfma_plan* plan, mlfma_info* info) {
+  if (!plan || !plan->p || !info) return fail(MLFMA_ERR_ARG, "null argument");
+  const mlfma::Plan& P = *plan->p;
+  std::memset(info, 0, sizeof(*info));
+  info->num_rwg = P.N;
+  info->num_unknowns = 2 * P.N;
+  info->max_level = P.maxL;
+  info->num_levels = P.maxL - 1;
+  for (int l = 2; l <= P.maxL && l - 2 < 16; ++l) {
+    info->boxes[l - 2] = P.lv[l].B;
+    info->L_k1[l - 2] = P.ml[0][l].L;
+    info->L_k2[l - 2] = P.ml[1][l].L;
+    info->K_k1[l - 2] = P.ml[0][l].K;
+    info->K_k2[l - 2] = P.ml[1][l].K;
+    info->far_pairs[l - 2] = P.lv[l].far_pairs;
+  }
+  info->near_pairs = P.near_pairs;
+  info->bytes_device = static_cast<double>(P.bytes);
+  info->setup_seconds = P.setup_seconds;
+  info->k1_re = P.k1.real();
+  info->k1_im = P.k1.imag();
+  info->k2_re = P.k2.real();
+  info->k2_im = P.k2.imag();
+  info->etai_re = P.etai.real();
+  info->etai_im = P.etai.imag();
+  info->wavelength = P.lambda;
+  return MLFMA_OK;
+}
+
+int mlfma_apply(mlfma_plan* plan, int n, const double* x, double* w) {
+  if (!plan || !plan->p || !x || !w) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    const size_t bytes = static_cast<size_t>(n) * sizeof(double2);
+    MLFMA_CUDA(cudaMemcpyAsync(P.d_x, x, bytes, cudaMemcpyHostToDevice, P.stream));
+    mlfma::apply_device(P, P.d_x, P.d_w, P.stream);
+    MLFMA_CUDA(cudaMemcpyAsync(w, P.d_w, bytes, cudaMemcpyDeviceToHost, P.stream));
+    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_apply_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream) {
+  if (!plan || !plan->p || !x_dev || !w_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (x_dev == w_dev) return fail(MLFMA_ERR_ARG, "x and w must not alias");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::apply_device(P, static_cast<const double2*>(x_dev), static_cast<double2*>(w_dev), s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_profile(mlfma_plan* plan, int on) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  plan->p->prof.on = on != 0;
+  plan->p->prof.used = 0;
+  return MLFMA_OK;
+}
+
+int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applies) {
+  if (!plan || !plan->p || !stage_ms) return fail(MLFMA_ERR_ARG, "null argument");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    MLFMA_CUDA(cudaSetDevice(plan->p->device));
+    const int n = mlfma::read_stage_times(*plan->p, stage_ms);
+    if (applies) *applies = n;
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_gmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr, double tol_abs,
+                double tol_rel, mlfma_solve_stats* stats, double* history, int history_cap) {
+  if (!plan || !plan->p || !x || !rhs) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (mr <= 0 || itr_max < 0) return fail(MLFMA_ERR_ARG, "mr must be positive, itr_max non-negative");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::SolveStats st;
+    std::vector<double> hist;
+    const bool ok = mlfma::gmres_solve(*plan->p, x, rhs, itr_max, mr, tol_abs, tol_rel, st, hist);
+    if (stats) {
+      stats->iterations = st.iterations;
+      stats->restarts = st.restarts;
+      stats->matvecs = st.matvecs;
+      stats->converged = ok ? 1 : 0;
+      stats->rel_residual = st.rel_residual;
+      stats->seconds = st.seconds;
+      stats->history_len = static_cast<int>(std::min<size_t>(hist.size(), history ? history_cap : 0));
+    }
+    if (history)
+      for (int i = 0; i < history_cap && i < static_cast<int>(hist.size()); ++i) history[i] = hist[i];
+    return ok ? MLFMA_OK : MLFMA_ERR_NOT_CONVERGED;
+  });
+}
+
+int mlfma_rhs_pmchwt(mlfma_plan* plan, const double kinc[3], const double einc[3], const double hinc[3],
+                     double* V) {
+  if (!plan || !plan->p || !kinc || !einc || !hinc || !V) return fail(MLFMA_ERR_ARG, "null argument");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::rhs_pmchwt(*plan->p, kinc, einc, hinc, V);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_rcs_pmchwt(mlfma_plan* plan, const double* I, int n_angles, const double* theta_deg,
+                     const double* phi_deg, double* field, double* rcs_db) {
+  if (!plan || !plan->p || !I || !theta_deg || !phi_deg || n_angles < 0)
+    return fail(MLFMA_ERR_ARG, "null argument");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::rcs_pmchwt(*plan->p, I, n_angles, theta_deg, phi_deg, field, rcs_db);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_get_rwgs(const mlfma_plan* plan, int* face_pos, int* face_neg, int* free_pos, int* free_neg,
+                   int* edge_a, int* edge_b, double* length, double* mid) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  const mlfma::Plan& P = *plan->p;
+  const mlfma::Rwg& R = P.rwg;
+  const mlfma::Mesh& M = P.mesh;
+  for (int i = 0; i < P.N; ++i) {
+    if (face_pos) face_pos[i] = M.face_id[R.fpos[i]];
+    if (face_neg) face_neg[i] = M.face_id[R.fneg[i]];
+    if (free_pos) free_pos[i] = M.point_id[R.free_pos[i]];
+    if (free_neg) free_neg[i] = M.point_id[R.free_neg[i]];
+    if (edge_a) edge_a[i] = M.point_id[R.ea[i]];
+    if (edge_b) edge_b[i] = M.point_id[R.eb[i]];
+    if (length) length[i] = R.len[i];
+    if (mid)
+      for (int a = 0; a < 3; ++a) mid[3 * i + a] = R.mid[3 * i + a];
+  }
+  return MLFMA_OK;
+}
+
+long long mlfma_get_level(const mlfma_plan* plan, int level, unsigned long long* morton, double* center) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  const mlfma::Plan& P = *plan->p;
+  if (level < 0 || level > P.maxL) return fail(MLFMA_ERR_ARG, "level out of range");
+  const mlfma::Level& L = P.tree.lv[level];
+  for (int b = 0; b < L.size(); ++b) {
+    if (morton) morton[b] = L.code[b];
+    if (center)
+      for (int a = 0; a < 3; ++a) center[3 * b + a] = L.center[3 * b + a];
+  }
+  return L.size();
+}
+
+long long mlfma_get_level_lists(const mlfma_plan* plan, int level, int* near_ptr, int* near_idx, int* far_ptr,
+                                int* far_idx, int* far_off) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  const mlfma::Plan& P = *plan->p;
+  if (level < 0 || level > P.maxL) return fail(MLFMA_ERR_ARG, "level out of range");
+  const mlfma::Level& L = P.tree.lv[level];
+  auto cp = [](const std::vector<int>& v, int* o) {
+    if (o) std::copy(v.begin(), v.end(), o);
+  };
+  cp(L.near_ptr, near_ptr);
+  cp(L.near_idx, near_idx);
+  cp(L.far_ptr, far_ptr);
+  cp(L.far_idx, far_idx);
+  cp(L.far_off, far_off);
+  return static_cast<long long>(L.far_idx.size());
+}
+
+long long mlfma_get_leaf_rwgs(const mlfma_plan* plan, int* leaf_ptr, int* leaf_rwg) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  const mlfma::Tree& T = plan->p->tree;
+  if (leaf_ptr) std::copy(T.leaf_ptr.begin(), T.leaf_ptr.end(), leaf_ptr);
+  if (leaf_rwg) std::copy(T.leaf_rwg.begin(), T.leaf_rwg.end(), leaf_rwg);
+  return static_cast<long long>(T.leaf_ptr.size()) - 1;
+}
+
+int mlfma_get_grid(const mlfma_plan* plan, int medium, int level, double* theta, double* phi, double* wtheta,
+                   double* wphi) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  const mlfma::Plan& P = *plan->p;
+  if (medium < 1 || medium > 2 || level < 2 || level > P.maxL) return fail(MLFMA_ERR_ARG, "range");
+  const mlfma::Grid& g = P.ml[medium - 1][level].grid;
+  if (theta) std::copy(g.theta.begin(), g.theta.end(), theta);
+  if (phi) std::copy(g.phi.begin(), g.phi.end(), phi);
+  if (wtheta) std::copy(g.wth.begin(), g.wth.end(), wtheta);
+  if (wphi) *wphi = g.wph;
+  return g.L;
+}
+
+int mlfma_get_interp(const mlfma_plan* plan, int medium, int level, int* tidx, double* lt, int* pidx,
+                     double* lp) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  const mlfma::Plan& P = *plan->p;
+  if (medium < 1 || medium > 2 || level < 2 || level >= P.maxL) return fail(MLFMA_ERR_ARG, "range");
+  const mlfma::Interp& I = P.ml[medium - 1][level].interp;
+  if (tidx) std::copy(I.tidx.begin(), I.tidx.end(), tidx);
+  if (lt) std::copy(I.lt.begin(), I.lt.end(), lt);
+  if (pidx) std::copy(I.pidx.begin(), I.pidx.end(), pidx);
+  if (lp) std::copy(I.lp.begin(), I.lp.end(), lp);
+  return MLFMA_OK;
+}
+
+long long mlfma_get_stage(mlfma_plan* plan, int which, int medium, int level, double* out) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  mlfma::Plan& P = *plan->p;
+  if (medium < 1 || medium > 2 || level < 2 || level > P.maxL || which < 0 || which > 1)
+    return fail(MLFMA_ERR_ARG, "range");
+  const mlfma::MediumLevel& M = P.ml[medium - 1][level];
+  const long long count = static_cast<long long>(P.lv[level].B) * 6 * M.K;
+  if (!out) return count;
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  const int st = guarded([&] {
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    MLFMA_CUDA(cudaMemcpy(out, which == 0 ? M.S : M.Bm, count * sizeof(double2), cudaMemcpyDeviceToHost));
+    return 0;
+  });
+  return st == 0 ? count : st;
+}
+
+long long mlfma_get_pattern(mlfma_plan* plan, int medium, int which, double* out) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  mlfma::Plan& P = *plan->p;
+  if (medium < 1 || medium > 2 || which < 0 || which > 1) return fail(MLFMA_ERR_ARG, "range");
+  const int K = P.ml[medium - 1][P.maxL].K;
+  const long long count = static_cast<long long>(P.N) * K * 3;
+  if (!out) return count;
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  int st = guarded([&] {
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    std::vector<double2> buf(static_cast<size_t>(count));
+    MLFMA_CUDA(cudaMemcpy(buf.data(), which == 0 ? P.d_Vs[medium - 1] : P.d_Vf[medium - 1],
+                          count * sizeof(double2), cudaMemcpyDeviceToHost));
+    // device [leaf order][3][K] -> [rwg id][K][3]
+    for (int r = 0; r < P.N; ++r) {
+      const int id = P.tree.leaf_rwg[r];
+      for (int c = 0; c < 3; ++c)
+        for (int k = 0; k < K; ++k) {
+          const double2 v = buf[(static_cast<size_t>(r) * 3 + c) * K + k];
+          const size_t o = (static_cast<size_t>(id) * K + k) * 3 + c;
+          out[2 * o] = v.x;
+          out[2 * o + 1] = v.y;
+        }
+    }
+    return 0;
+  });
+  return st == 0 ? count : st;
+}
+
+long long mlfma_get_transfer(mlfma_plan* plan, int medium, int level, int* offsets, double* tf) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  mlfma::Plan& P = *plan->p;
+  if (medium < 1 || medium > 2 || level < 2 || level > P.maxL) return fail(MLFMA_ERR_ARG, "range");
+  const mlfma::MediumLevel& M = P.ml[medium - 1][level];
+  const long long count = static_cast<long long>(M.nvec) * M.K;
+  if (offsets)
+    for (int v = 0; v < M.nvec; ++v) {
+      int dx, dy, dz;
+      mlfma::decode_offset(M.vec_off[v], dx, dy, dz);
+      offsets[3 * v] = dx;
+      offsets[3 * v + 1] = dy;
+      offsets[3 * v + 2] = dz;
+    }
+  if (!tf) return count;
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  int st = guarded([&] {
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    std::vector<double> rhat;
+    std::vector<int> hoff, hL;
+    std::vector<double2> h2;
+    P.tf_inputs(medium - 1, level, rhat, hoff, hL, h2);
+    double2* tmp = nullptr;
+    MLFMA_CUDA(cudaMalloc(&tmp, std::max<long long>(count, 1) * sizeof(double2)));
+    mlfma::launch_transfer(P, medium - 1, level, rhat, hoff, hL, h2, false, tmp, P.stream);
+    cudaError_t e = cudaMemcpy(tf, tmp, count * sizeof(double2), cudaMemcpyDeviceToHost);
+    cudaFree(tmp);
+    MLFMA_CUDA(e);
+    return 0;
+  });
+  return st == 0 ? count : st;
+}
+
+long long mlfma_get_near(mlfma_plan* plan, int* target, int* source, double* z11, double* z12, double* z22) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  mlfma::Plan& P = *plan->p;
+  const mlfma::Tree& T = P.tree;
+  const int B = T.lv[P.maxL].size();
+  if (target || source) {
+    long long e = 0;
+    for (int b = 0; b < B; ++b)
+      for (int t = T.leaf_ptr[b]; t < T.leaf_ptr[b + 1]; ++t)
+        for (int j = P.h_near_sptr[b]; j < P.h_near_sptr[b + 1]; ++j, ++e) {
+          if (target) target[e] = T.leaf_rwg[t];
+          if (source) source[e] = P.h_near_src[j];
+        }
+  }
+  if (!z11 && !z12 && !z22) return P.near_pairs;
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  int st = guarded([&] {
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    std::vector<double2> buf(3 * static_cast<size_t>(P.near_pairs));
+    MLFMA_CUDA(cudaMemcpy(buf.data(), P.d_near_z, buf.size() * sizeof(double2), cudaMemcpyDeviceToHost));
+    for (long long e = 0; e < P.near_pairs; ++e) {
+      double* outs[3] = {z11, z12, z22};
+      for (int q = 0; q < 3; ++q)
+        if (outs[q]) {
+          outs[q][2 * e] = buf[3 * e + q].x;
+          outs[q][2 * e + 1] = buf[3 * e + q].y;
+        }
+    }
+    return 0;
+  });
+  return st == 0 ? P.near_pairs : st;
+}
+
+}  // extern "C"

@@ -1,0 +1,44 @@
+// complex128 helpers on double2 (x = real, y = imaginary).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace mlfma {
+
+__host__ __device__ __forceinline__ double2 c2(double re, double im) { return make_double2(re, im); }
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cneg(double2 a) { return make_double2(-a.x, -a.y); }
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// a * b + c
+__host__ __device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+// s * a + c (s real)
+__host__ __device__ __forceinline__ double2 cfmas(double s, double2 a, double2 c) {
+  return make_double2(fma(s, a.x, c.x), fma(s, a.y, c.y));
+}
+__host__ __device__ __forceinline__ double2 cmulj(double2 a) { return make_double2(-a.y, a.x); }  // j * a
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  // Smith's algorithm
+  if (fabs(b.x) >= fabs(b.y)) {
+    const double r = b.y / b.x, d = b.x + b.y * r;
+    return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  }
+  const double r = b.x / b.y, d = b.x * r + b.y;
+  return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+__device__ __forceinline__ double2 cexp(double2 z) {
+  double s, c;
+  sincos(z.y, &s, &c);
+  const double e = exp(z.x);
+  return make_double2(e * c, e * s);
+}
+// exp(-j * k * t) for complex k and real t
+__device__ __forceinline__ double2 cexp_mjkt(double2 k, double t) {
+  return cexp(make_double2(k.y * t, -k.x * t));
+}
+
+}  // namespace mlfma

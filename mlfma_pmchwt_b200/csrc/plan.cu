@@ -1,0 +1,287 @@
+// Plan construction: host tables, device upload, device setup kernels.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <map>
+
+#include "cplx.cuh"
+#include "plan.hpp"
+
+namespace mlfma {
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+Plan::~Plan() {
+  if (device >= 0) {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& set : prof.sets)
+      for (cudaEvent_t e : set) cudaEventDestroy(e);
+    for (void* p : allocations) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+}
+
+namespace {
+
+std::vector<double> soa3(const std::vector<double>& aos, int K) {
+  std::vector<double> out(3 * static_cast<size_t>(K));
+  for (int k = 0; k < K; ++k)
+    for (int a = 0; a < 3; ++a) out[static_cast<size_t>(a) * K + k] = aos[3 * static_cast<size_t>(k) + a];
+  return out;
+}
+
+// exp(-j k khat.d) for the 8 child octants, d = child centre - parent centre
+// (sign = +1) or parent - child (sign = -1); child edge h.
+std::vector<double2> shift_table(const Grid& g, cplx k, double h, double sign) {
+  std::vector<double2> t(8 * static_cast<size_t>(g.K));
+  const cplx J(0.0, 1.0);
+  for (int o = 0; o < 8; ++o) {
+    const double d[3] = {sign * (((o & 1) ? 0.5 : -0.5) * h), sign * (((o & 2) ? 0.5 : -0.5) * h),
+                         sign * (((o & 4) ? 0.5 : -0.5) * h)};
+    for (int kk = 0; kk < g.K; ++kk) {
+      const double* kp = &g.khat[3 * static_cast<size_t>(kk)];
+      const cplx kr = k * (kp[0] * d[0] + kp[1] * d[1] + kp[2] * d[2]);
+      const cplx e = std::exp(-J * kr);
+      t[static_cast<size_t>(o) * g.K + kk] = make_double2(e.real(), e.imag());
+    }
+  }
+  return t;
+}
+
+}  // namespace
+
+std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
+  const auto t0 = std::chrono::steady_clock::now();
+  auto P = std::make_unique<Plan>();
+  P->device = prm.device;
+  P->verbose = prm.verbose;
+  P->mesh = std::move(mesh);
+  if (!(prm.freq > 0) || !(prm.leaf_coeff > 0)) throw std::invalid_argument("freq and leaf_coeff must be positive");
+  if (!quad_rule(prm.gauss, P->quad)) throw std::invalid_argument("unsupported triangle rule");
+  std::string err;
+  if (!build_rwgs(P->mesh, P->rwg, err)) throw std::domain_error(err);
+  P->N = P->rwg.N;
+
+  // Wave constants (Code/EMSource.cpp:6-32).
+  P->freq = prm.freq;
+  P->lambda = kC0 / prm.freq;
+  const double k = 2.0 * kPi / P->lambda;
+  P->epsr = prm.epsr;
+  P->mur = prm.mur;
+  P->k1 = cplx(k, 0.0);
+  P->k2 = cplx(k, 0.0) * std::sqrt(prm.epsr * prm.mur);
+  P->etai = std::sqrt(prm.mur / prm.epsr);
+  P->eta1 = cplx(kEta0, 0.0);
+  P->eta2 = cplx(kEta0, 0.0) * std::sqrt(prm.mur / prm.epsr);
+
+  build_tree(P->rwg, prm.leaf_coeff * P->lambda, P->tree);
+  Tree& T = P->tree;
+  const int L = T.maxLevel;
+  P->maxL = L;
+  const double kabs[2] = {std::abs(P->k1), std::abs(P->k2)};
+  const cplx kc[2] = {P->k1, P->k2};
+  for (int m = 0; m < 2; ++m) {
+    P->ml[m].assign(L + 1, MediumLevel());
+    for (int l = 2; l <= L; ++l) {
+      MediumLevel& M = P->ml[m][l];
+      M.grid = build_grid(kabs[m], T.lv[l].len);
+      M.L = M.grid.L;
+      M.nth = M.grid.nth;
+      M.nph = M.grid.nph;
+      M.K = M.grid.K;
+    }
+    for (int l = 2; l < L; ++l) P->ml[m][l].interp = build_interp(P->ml[m][l].grid, P->ml[m][l + 1].grid);
+  }
+  P->lv.assign(L + 1, DevLevel());
+  for (int l = 0; l <= L; ++l) {
+    P->lv[l].B = T.lv[l].size();
+    P->lv[l].far_pairs = static_cast<long long>(T.lv[l].far_idx.size());
+  }
+  // near-field source lists per leaf box: near neighbours (list order), then self
+  {
+    const Level& Lf = T.lv[L];
+    const int B = Lf.size();
+    P->h_near_sptr.assign(B + 1, 0);
+    P->h_near_zoff.assign(B + 1, 0);
+    P->h_near_src.clear();
+    for (int b = 0; b < B; ++b) {
+      for (int e = Lf.near_ptr[b]; e <= Lf.near_ptr[b + 1]; ++e) {
+        const int nb = e < Lf.near_ptr[b + 1] ? Lf.near_idx[e] : b;
+        for (int q = T.leaf_ptr[nb]; q < T.leaf_ptr[nb + 1]; ++q) P->h_near_src.push_back(T.leaf_rwg[q]);
+      }
+      P->h_near_sptr[b + 1] = static_cast<int>(P->h_near_src.size());
+      const long long nt = T.leaf_ptr[b + 1] - T.leaf_ptr[b];
+      const long long ns = P->h_near_sptr[b + 1] - P->h_near_sptr[b];
+      P->h_near_zoff[b + 1] = P->h_near_zoff[b] + nt * ns;
+    }
+    P->near_pairs = P->h_near_zoff[B];
+  }
+  if (prm.device < 0) {  // host-only plan: tables for inspection, no device work
+    P->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return P;
+  }
+
+  // ------------------------------------------------------------- device
+  MLFMA_CUDA(cudaSetDevice(prm.device));
+  MLFMA_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+  cudaStream_t s = P->stream;
+  const Mesh& Me = P->mesh;
+  const Rwg& R = P->rwg;
+  P->d_xyz = P->upload(Me.xyz);
+  P->d_face_v = P->upload(Me.face_v);
+  P->d_face_id = P->upload(Me.face_id);
+  P->d_face_area = P->upload(Me.area);
+  P->d_face_normal = P->upload(Me.normal);
+  P->d_rwg_fpos = P->upload(R.fpos);
+  P->d_rwg_fneg = P->upload(R.fneg);
+  P->d_rwg_vpos = P->upload(R.free_pos);
+  P->d_rwg_vneg = P->upload(R.free_neg);
+  P->d_rwg_len = P->upload(R.len);
+
+  for (int l = 0; l <= L; ++l) {
+    const Level& Lv = T.lv[l];
+    DevLevel& D = P->lv[l];
+    if (l < L) D.child_begin = P->upload(Lv.child_begin);
+    D.parent = P->upload(Lv.parent);
+    std::vector<int> oct(Lv.size());
+    for (int b = 0; b < Lv.size(); ++b) oct[b] = (Lv.ix[b] & 1) | ((Lv.iy[b] & 1) << 1) | ((Lv.iz[b] & 1) << 2);
+    D.octant = P->upload(oct);
+    if (l >= 2) {
+      D.far_ptr = P->upload(Lv.far_ptr);
+      D.far_idx = P->upload(Lv.far_idx);
+      D.far_off = P->upload(Lv.far_off);
+    }
+  }
+  for (int m = 0; m < 2; ++m) {
+    for (int l = 2; l <= L; ++l) {
+      MediumLevel& M = P->ml[m][l];
+      const int B = P->lv[l].B;
+      M.khat = P->upload(soa3(M.grid.khat, M.K));
+      M.S = P->alloc<double2>(static_cast<size_t>(B) * 6 * M.K);
+      M.Bm = P->alloc<double2>(static_cast<size_t>(B) * 6 * M.K);
+      if (l < L) {
+        const Interp& I = M.interp;
+        M.tidx = P->upload(I.tidx);
+        M.lt = P->upload(I.lt);
+        M.pidx = P->upload(I.pidx);
+        M.lp = P->upload(I.lp);
+        const double hc = T.lv[l + 1].len;
+        M.ph_up = P->upload(shift_table(M.grid, kc[m], hc, -1.0));  // parent - child
+        M.ph_dn = P->upload(shift_table(M.grid, kc[m], hc, +1.0));  // child - parent
+      }
+      if (l > 2) {
+        // transposed interpolation: child direction <- (parent direction, weight)
+        const MediumLevel& Pm = P->ml[m][l - 1];
+        const Interp& I = Pm.interp;
+        std::vector<int> cnt(M.K + 1, 0);
+        for (int kp = 0; kp < Pm.K; ++kp) {
+          const int t = kp / Pm.nph, p = kp % Pm.nph;
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) cnt[I.tidx[3 * t + i] * M.nph + I.pidx[3 * p + j] + 1]++;
+        }
+        for (int kk = 0; kk < M.K; ++kk) cnt[kk + 1] += cnt[kk];
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1), kps(cnt[M.K]);
+        std::vector<double> ws(cnt[M.K]);
+        for (int kp = 0; kp < Pm.K; ++kp) {
+          const int t = kp / Pm.nph, p = kp % Pm.nph;
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+              const int c = I.tidx[3 * t + i] * M.nph + I.pidx[3 * p + j];
+              kps[fill[c]] = kp;
+              ws[fill[c]] = I.lt[3 * t + i] * I.lp[3 * p + j];
+              fill[c]++;
+            }
+        }
+        M.tr_ptr = P->upload(cnt);
+        M.tr_kp = P->upload(kps);
+        M.tr_w = P->upload(ws);
+      }
+      // transfer factors over the offsets this level uses (Code/AlgoMLFMM.h:192-295)
+      {
+        std::vector<char> used(343, 0);
+        for (int e : T.lv[l].far_off) used[e] = 1;
+        std::vector<int> off2vec(343, -1);
+        M.vec_off.clear();
+        for (int e = 0; e < 343; ++e)
+          if (used[e]) {
+            off2vec[e] = static_cast<int>(M.vec_off.size());
+            M.vec_off.push_back(e);
+          }
+        M.nvec = static_cast<int>(M.vec_off.size());
+        M.off2vec = P->upload(off2vec);
+        std::vector<double> rhat;
+        std::vector<int> hoff, hL;
+        std::vector<double2> h2all;
+        P->tf_inputs(m, l, rhat, hoff, hL, h2all);
+        M.tfw = P->alloc<double2>(static_cast<size_t>(std::max(M.nvec, 1)) * M.K);
+        launch_transfer(*P, m, l, rhat, hoff, hL, h2all, true, M.tfw, s);
+      }
+    }
+  }
+  // leaf data
+  {
+    const Level& Lf = T.lv[L];
+    P->d_leaf_ptr = P->upload(T.leaf_ptr);
+    P->d_leaf_rwg = P->upload(T.leaf_rwg);
+    P->d_rwg_leafbox = P->upload(T.rwg_leaf);
+    P->d_leaf_center = P->upload(Lf.center);
+    for (int m = 0; m < 2; ++m) {
+      const int K = P->ml[m][L].K;
+      P->d_Vs[m] = P->alloc<double2>(static_cast<size_t>(P->N) * 3 * K);
+      P->d_Vf[m] = P->alloc<double2>(static_cast<size_t>(P->N) * 3 * K);
+      launch_patterns(*P, m, s);
+    }
+  }
+  // near field
+  {
+    std::vector<double> q(4 * static_cast<size_t>(P->quad.n));
+    P->d_near_sptr = P->upload(P->h_near_sptr);
+    P->d_near_src = P->upload(P->h_near_src);
+    P->d_near_zoff = P->upload(P->h_near_zoff);
+    P->d_near_z = P->alloc<double2>(3 * static_cast<size_t>(std::max<long long>(P->near_pairs, 1)));
+    launch_near(*P, s);
+  }
+  P->d_x = P->alloc<double2>(2 * static_cast<size_t>(P->N));
+  P->d_w = P->alloc<double2>(2 * static_cast<size_t>(P->N));
+  MLFMA_CUDA(cudaStreamSynchronize(s));
+  P->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (P->verbose) {
+    std::fprintf(stderr, "mlfma: N=%d maxLevel=%d near pairs=%lld device bytes=%.3e setup %.3f s\n", P->N, L,
+                 P->near_pairs, static_cast<double>(P->bytes), P->setup_seconds);
+  }
+  return P;
+}
+
+// Inputs of the transfer-factor kernel for (medium, level): per used offset,
+// the unit vector, h2_l(|k R|) for l <= min(L, ceil(|k R|)) (Code/AlgoMLFMM.h:252-267).
+void Plan::tf_inputs(int m, int l, std::vector<double>& rhat, std::vector<int>& hoff, std::vector<int>& hL,
+                     std::vector<double2>& h2all) const {
+  const MediumLevel& M = ml[m][l];
+  const cplx kw = m == 0 ? k1 : k2;
+  const double len = tree.lv[l].len;
+  rhat.clear();
+  hoff.clear();
+  hL.clear();
+  h2all.clear();
+  std::vector<cplx> h2;
+  for (int e : M.vec_off) {
+    int dx, dy, dz;
+    decode_offset(e, dx, dy, dz);
+    double r[3] = {dx * len, dy * len, dz * len};
+    const double Rpq = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    for (double& v : r) v /= Rpq;
+    const cplx kR = kw * Rpq;
+    const int Lt = std::min(M.L, static_cast<int>(std::ceil(std::abs(kR))));
+    hankel2_array(Lt, std::abs(kR), h2);
+    rhat.insert(rhat.end(), r, r + 3);
+    hoff.push_back(static_cast<int>(h2all.size()));
+    hL.push_back(Lt);
+    for (const cplx& v : h2) h2all.push_back(make_double2(v.real(), v.imag()));
+  }
+}
+
+}  // namespace mlfma

@@ -1,0 +1,170 @@
+// Device-resident PMCHWT MLFMA operator ("plan") and the kernels that build
+// and apply it. Layout in HBM (per medium m = k1 | k2, per level l):
+//   S_m,l / B_m,l : [box][6][K_m,l] complex128 (J x,y,z then M x,y,z),
+//                   boxes in Morton order; K directions theta-major.
+//   radiation / receive leaf patterns: [rwg in leaf order][3][K_m,leaf].
+//   transfer factors: [vec][K] complex128 with the quadrature weight folded in.
+//   near field: per leaf box b, a dense block [n_b targets][sources of the
+//               27-neighbourhood][3] complex128 (z11, z12, z22; z21 = -z12).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <complex>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "host.hpp"
+
+namespace mlfma {
+
+struct MediumLevel {
+  int L = 0, nth = 0, nph = 0, K = 0;
+  double2* S = nullptr;
+  double2* Bm = nullptr;
+  double2* tfw = nullptr;      // [nvec][K], weights folded in
+  int nvec = 0;
+  int* off2vec = nullptr;      // [343] -> vec index or -1
+  double* khat = nullptr;      // [3][K] (x row, y row, z row)
+  // this level as parent of level+1
+  int* tidx = nullptr;         // [nth][3] into the child theta grid
+  double* lt = nullptr;        // [nth][3]
+  int* pidx = nullptr;         // [nph][3] into the child phi grid
+  double* lp = nullptr;        // [nph][3]
+  double2* ph_up = nullptr;    // [8][K]: exp(-j k khat.(c_parent - c_child)), child octant o
+  double2* ph_dn = nullptr;    // [8][K]: exp(-j k khat.(c_child - c_parent))
+  // this level as child of level-1: for each child direction, the parent
+  // directions that interpolate onto it and the Lagrange weight
+  int* tr_ptr = nullptr;       // [K+1]
+  int* tr_kp = nullptr;
+  double* tr_w = nullptr;
+  // host copies
+  Grid grid;
+  Interp interp;               // this level from level+1 (levels 2..maxL-1)
+  std::vector<int> vec_off;    // encoded offset of each vec
+};
+
+struct DevLevel {
+  int B = 0;
+  int* child_begin = nullptr;  // [B+1] into level+1
+  int* parent = nullptr;       // [B]
+  int* octant = nullptr;       // [B] position in the parent cube
+  int* far_ptr = nullptr;      // [B+1]
+  int* far_idx = nullptr;
+  int* far_off = nullptr;
+  long long far_pairs = 0;
+};
+
+// Per-apply CUDA events between stage groups, recorded on the launching
+// stream: [m1 agg | m1 up | m1 down | m2 agg | m2 up | m2 down | leaf_out].
+struct StageProfiler {
+  static constexpr int kEvents = 8;
+  bool on = false;
+  std::vector<std::array<cudaEvent_t, kEvents>> sets;
+  size_t used = 0;
+};
+
+struct Plan {
+  // ---- host description
+  Mesh mesh;
+  Rwg rwg;
+  Tree tree;
+  Quad quad;
+  int N = 0;
+  int maxL = 0;
+  int device = 0;
+  int verbose = 0;
+  cplx k1, k2, eta1, eta2, etai, epsr, mur;
+  double lambda = 0.0, freq = 0.0;
+  double setup_seconds = 0.0;
+  std::vector<MediumLevel> ml[2];   // index = physical level (0..maxL), used 2..maxL
+  std::vector<DevLevel> lv;         // index = physical level
+  // ---- device geometry
+  double* d_xyz = nullptr;          // [3 * points]
+  int* d_face_v = nullptr;          // [3 * faces]
+  int* d_face_id = nullptr;
+  double* d_face_area = nullptr;
+  double* d_face_normal = nullptr;  // [3 * faces]
+  int* d_rwg_fpos = nullptr;
+  int* d_rwg_fneg = nullptr;
+  int* d_rwg_vpos = nullptr;
+  int* d_rwg_vneg = nullptr;
+  double* d_rwg_len = nullptr;
+  double* d_quad = nullptr;         // [4][nq]: l1, l2, l3, w
+  // ---- leaf data
+  int* d_leaf_ptr = nullptr;        // [Bleaf+1] into leaf order
+  int* d_leaf_rwg = nullptr;        // leaf order -> RWG id
+  int* d_rwg_leafbox = nullptr;     // [N] leaf box of each RWG id
+  double* d_leaf_center = nullptr;  // [3 * Bleaf]
+  double2* d_Vs[2] = {nullptr, nullptr};   // radiation patterns [N][3][K]
+  double2* d_Vf[2] = {nullptr, nullptr};   // receive patterns
+  // ---- near field
+  std::vector<long long> h_near_zoff;      // per leaf box, offset of its block (pairs)
+  std::vector<int> h_near_sptr;            // per leaf box, offset into source list
+  std::vector<int> h_near_src;             // concatenated source RWG ids per leaf box
+  int* d_near_sptr = nullptr;       // [Bleaf+1]
+  int* d_near_src = nullptr;        // concatenated source RWG ids per box
+  long long* d_near_zoff = nullptr; // [Bleaf+1]
+  double2* d_near_z = nullptr;      // [pairs][3]
+  long long near_pairs = 0;
+  // ---- vectors
+  double2* d_x = nullptr;           // staging for host-pointer apply
+  double2* d_w = nullptr;
+  cudaStream_t stream = nullptr;
+  StageProfiler prof;
+  size_t bytes = 0;
+  std::vector<void*> allocations;
+
+  ~Plan();
+  void tf_inputs(int m, int l, std::vector<double>& rhat, std::vector<int>& hoff, std::vector<int>& hL,
+                 std::vector<double2>& h2all) const;
+  template <class T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocations.push_back(p);
+    bytes += count * sizeof(T);
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* upload(const std::vector<T>& v) {
+    T* p = alloc<T>(v.size());
+    if (!v.empty()) {
+      cudaError_t e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+    }
+    return p;
+  }
+};
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+void check_cuda(cudaError_t e, const char* what);
+#define MLFMA_CUDA(call) ::mlfma::check_cuda((call), #call)
+
+// Setup (plan.cu)
+struct PlanParams {
+  double freq = 3.0e8;
+  cplx epsr{1.0, 0.0}, mur{1.0, 0.0};
+  double leaf_coeff = 0.3;
+  int gauss = 7;
+  int device = 0;
+  int verbose = 0;
+};
+std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& p);
+
+// Device work (setup_kernels.cu / matvec_kernels.cu)
+void launch_patterns(Plan& P, int medium, cudaStream_t s);
+void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& rhat,
+                     const std::vector<int>& hoff, const std::vector<int>& hL,
+                     const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s);
+void launch_near(Plan& P, cudaStream_t s);
+void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s);
+int read_stage_times(Plan& P, double out[4]);
+
+}  // namespace mlfma

@@ -1,0 +1,27 @@
+// Krylov solve, excitation and far field on the device.
+#pragma once
+#include <vector>
+
+#include "plan.hpp"
+
+namespace mlfma {
+
+struct SolveStats {
+  int iterations = 0;
+  int restarts = 0;
+  int matvecs = 0;
+  double rel_residual = 0.0;
+  double seconds = 0.0;
+};
+
+// Restarted GMRES(mr) of Code/GMRES.h:65-217 on the device operator; x, rhs
+// host complex128 [2N]. Returns true when converged.
+bool gmres_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, double tol_abs, double tol_rel,
+                 SolveStats& st, std::vector<double>& history);
+
+void rhs_pmchwt(Plan& P, const double kinc[3], const double einc[3], const double hinc[3], double* V);
+
+void rcs_pmchwt(Plan& P, const double* I, int n_angles, const double* theta_deg, const double* phi_deg,
+                double* field, double* rcs_db);
+
+}  // namespace mlfma

@@ -1,0 +1,204 @@
+"""GPU parity of the product against the reference compiled from its sources.
+
+Every call goes through the C ABI (libmlfma_pmchwt.so via the Python
+mirror). Tolerances:
+  * matvec: relative 2-norm <= 1e-10 per matvec (the plain FP64 bar);
+  * setup tables (patterns, transfer factors, near field): relative 2-norm
+    <= 1e-11 (their rounding feeds the matvec);
+  * RCS: |dB difference| <= 0.01 dB on identical currents.
+"""
+import numpy as np
+import pytest
+
+from conftest import FREQ, needs_lib, needs_oracle, rel
+
+pytestmark = [pytest.mark.gpu, needs_lib, needs_oracle]
+
+MATVEC_TOL = 1e-10
+TABLE_TOL = 1e-11
+
+_ops = {}
+
+
+def gpu_op(case_files, name):
+    from mlfma_pmchwt_b200 import MLFMM
+    if name not in _ops:
+        m, p, eps, leaf = case_files[name]
+        _ops[name] = MLFMM(m, freq=FREQ, eps_r=eps, leaf_coeff=leaf, device=0)
+    return _ops[name]
+
+
+CASES = ["sphere_s2", "sphere_s3", "sphere_s3_lossy", "ellipsoid_s3"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_leaf_patterns(case_files, ref_ops, name):
+    op, ref = gpu_op(case_files, name), ref_ops(name)
+    for med in (1, 2):
+        for w in ("s", "f"):
+            assert rel(op.pattern(med, w), ref.pattern(med, w)) < TABLE_TOL, (med, w)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_transfer_factors(case_files, ref_ops, name):
+    op, ref = gpu_op(case_files, name), ref_ops(name)
+    for med in (1, 2):
+        for lvl in range(2, op.max_level + 1):
+            tf, offs = op.transfer(med, lvl)
+            rtf, rvec = ref.transfer(med, lvl)
+            box = ref.level(lvl)["length"][0]
+            roffs = np.rint(rvec / box).astype(int)
+            assert {tuple(o) for o in offs} == {tuple(o) for o in roffs}
+            where = {tuple(o): i for i, o in enumerate(offs)}
+            sel = np.array([where[tuple(o)] for o in roffs])
+            assert rel(tf[sel], rtf) < TABLE_TOL, (med, lvl)
+
+
+def _dense_near(op, ref):
+    nr = op.near()
+    ptr, ids, vals = ref.znear()
+    N = op.N
+    mine = {}
+    for t, s, a, b, c in zip(nr["target"], nr["source"], nr["z11"], nr["z12"], nr["z22"]):
+        mine[(int(t), int(s))] = (a, b, -b, c)
+    got, want = [], []
+    for t in range(N):
+        r1 = slice(ptr[t], ptr[t + 1])
+        r2 = slice(ptr[N + t], ptr[N + t + 1])
+        ids1, v1, v2 = ids[r1], vals[r1], vals[r2]
+        for j in range(0, len(ids1), 2):
+            s = int(ids1[j])
+            got.extend(mine[(t, s)])
+            want.extend((v1[j], v1[j + 1], v2[j], v2[j + 1]))
+    return np.array(got), np.array(want), len(mine)
+
+
+@pytest.mark.parametrize("name", ["sphere_s2", "sphere_s3_lossy"])
+def test_near_field_entries(case_files, ref_ops, name):
+    op, ref = gpu_op(case_files, name), ref_ops(name)
+    got, want, pairs = _dense_near(op, ref)
+    assert pairs == op.info.near_pairs and len(want) == 4 * pairs
+    assert rel(got, want) < TABLE_TOL
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_matvec_matches_reference(case_files, ref_ops, name):
+    from mlfma_pmchwt_b200 import mesh as M
+    op, ref = gpu_op(case_files, name), ref_ops(name)
+    x = M.unit_disk_vector(op.n, 0)
+    err = rel(op.apply_ax(x), ref.apply(x))
+    assert err < MATVEC_TOL, err
+    # a second, unrelated vector and the all-ones vector of the reference's export design
+    rng = np.random.default_rng(11)
+    y = rng.standard_normal(op.n) + 1j * rng.standard_normal(op.n)
+    assert rel(op.apply_ax(y), ref.apply(y)) < MATVEC_TOL
+    ones = np.ones(op.n, dtype=complex)
+    assert rel(op.apply_ax(ones), ref.apply(ones)) < MATVEC_TOL
+
+
+@pytest.mark.parametrize("name", ["sphere_s3"])
+def test_stage_arrays(case_files, ref_ops, name):
+    """Aggregated (Sm) and incoming (Bm) patterns per level and box."""
+    from mlfma_pmchwt_b200 import mesh as M
+    op, ref = gpu_op(case_files, name), ref_ops(name)
+    x = M.unit_disk_vector(op.n, 3)
+    op.apply_ax(x)
+    ref.apply(x)
+    for med in (1, 2):
+        for lvl in range(2, op.max_level + 1):
+            codes, _ = op.level(lvl)
+            where = {int(c): i for i, c in enumerate(codes)}
+            rl = ref.level(lvl)
+            S, B = op.stage("S", med, lvl), op.stage("B", med, lvl)
+            got_s, want_s, got_b, want_b = [], [], [], []
+            for bi, code in enumerate(rl["morton"]):
+                mi = where[int(code)]
+                for pm in (0, 1):
+                    got_s.append(S[mi, 3 * pm:3 * pm + 3, :].T)
+                    want_s.append(ref.stage("S", med, lvl, bi, pm))
+                    got_b.append(B[mi, 3 * pm:3 * pm + 3, :].T)
+                    want_b.append(ref.stage("B", med, lvl, bi, pm))
+            assert rel(np.array(got_s), np.array(want_s)) < MATVEC_TOL, ("S", med, lvl)
+            assert rel(np.array(got_b), np.array(want_b)) < MATVEC_TOL, ("B", med, lvl)
+
+
+def test_device_apply_equals_host_apply(case_files):
+    import torch
+    from mlfma_pmchwt_b200 import mesh as M
+    op = gpu_op(case_files, "sphere_s3")
+    x = M.unit_disk_vector(op.n, 5)
+    xd = torch.from_numpy(x).cuda()
+    wd = torch.empty_like(xd)
+    op.apply_device(xd.data_ptr(), wd.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(wd.cpu().numpy(), op.apply_ax(x))
+
+
+def test_linearity_and_determinism(case_files):
+    from mlfma_pmchwt_b200 import mesh as M
+    op = gpu_op(case_files, "ellipsoid_s3")
+    a, b = M.unit_disk_vector(op.n, 1), M.unit_disk_vector(op.n, 2)
+    alpha, beta = 0.3 - 1.1j, -2.0 + 0.5j
+    lhs = op.apply_ax(alpha * a + beta * b)
+    rhs = alpha * op.apply_ax(a) + beta * op.apply_ax(b)
+    assert rel(lhs, rhs) < 1e-13
+    np.testing.assert_array_equal(op.apply_ax(a), op.apply_ax(a))  # bitwise reproducible
+
+
+@pytest.mark.parametrize("name", ["sphere_s3", "sphere_s3_lossy"])
+def test_rhs_and_rcs(case_files, ref_ops, name):
+    from mlfma_pmchwt_b200 import mesh as M, plane_wave
+    op, ref = gpu_op(case_files, name), ref_ops(name)
+    for pol, th, ph in ((0.0, 0.0, 0.0), (90.0, 30.0, 45.0), (0.0, 180.0, 0.0)):
+        k, e, h = plane_wave(pol, th, ph)
+        Vr, vecs = ref.rhs(pol, th, ph)
+        np.testing.assert_array_equal(np.array([k, e, h]), vecs)
+        assert rel(op.compute_v_pmchwt(k, e, h), Vr) < 1e-13
+    I = M.unit_disk_vector(op.n, 9)
+    th = np.arange(0.0, 180.01, 0.5)
+    field, db = op.calculate_rcs_pmchwt(I, th, 0.0)
+    for i in range(0, len(th), 24):
+        fr, dbr = ref.rcs(I, 0.0, th[i], 0.0)
+        assert rel(field[i], fr) < 1e-12
+        assert np.max(np.abs(db[i] - dbr)) < 0.01
+
+
+def test_gmres_history_matches_reference(case_files, ref_ops):
+    """GMRES(30) from x0 = 0 on the plane-wave excitation: the residual
+    estimates of the first 60 inner steps and the iterate agree with the
+    reference's own solve (MLFMM::matrix_solver -> MGMRES::mgmres)."""
+    from mlfma_pmchwt_b200 import plane_wave
+    op, ref = gpu_op(case_files, "sphere_s2"), ref_ops("sphere_s2")
+    V = op.compute_v_pmchwt(*plane_wave(0.0, 0.0, 0.0))
+    x, st = op.matrix_solver(V, itr_max=60, mr=30, tol_abs=1e-8, tol_rel=1e-6)
+    xr, info = ref.solve(V, itr_max=60, mr=30, tol_abs=1e-8, tol_rel=1e-6)
+    h, hr = st["history"], np.array(info["history"])
+    assert len(h) == len(hr) > 0
+    np.testing.assert_allclose(h, hr, rtol=1e-4)  # the reference prints 6 digits
+    assert rel(x, xr) < 1e-7
+    r = np.linalg.norm(ref.apply(x) - V) / np.linalg.norm(V)
+    assert abs(r - st["rel_residual"]) < 1e-9
+
+
+def test_solve_to_convergence_and_rcs(case_files, ref_ops):
+    """Small body solved to 1e-6 by both; bistatic RCS (361 angles) within 0.01 dB."""
+    from mlfma_pmchwt_b200 import plane_wave
+    op, ref = gpu_op(case_files, "sphere_s2"), ref_ops("sphere_s2")
+    V = op.compute_v_pmchwt(*plane_wave(0.0, 0.0, 0.0))
+    x, st = op.matrix_solver(V, itr_max=2000, mr=50, tol_abs=1e-12, tol_rel=1e-6)
+    xr, info = ref.solve(V, itr_max=2000, mr=50, tol_abs=1e-12, tol_rel=1e-6)
+    assert st["converged"] and st["rel_residual"] < 1e-6
+    th = np.arange(0.0, 180.01, 0.5)
+    _, db = op.calculate_rcs_pmchwt(x, th, 0.0)
+    dbr = np.array([ref.rcs(xr, 0.0, t, 0.0)[1] for t in th])
+    assert np.max(np.abs(db - dbr)) < 0.01
+
+
+def test_error_paths_on_device_plan(case_files):
+    from mlfma_pmchwt_b200 import MlfmaError
+    op = gpu_op(case_files, "sphere_s2")
+    with pytest.raises(ValueError):
+        op.apply_ax(np.zeros(op.n - 2, complex))
+    with pytest.raises(MlfmaError) as e:
+        op.apply_device(0, 0)
+    assert e.value.code == -1

@@ -1,0 +1,52 @@
+"""Synthetic mesh generator, NAS round trip and the seeded vector generator."""
+import numpy as np
+import pytest
+
+from mlfma_pmchwt_b200 import mesh as M
+
+
+@pytest.mark.parametrize("sub,faces,edges", [(0, 20, 30), (3, 1280, 1920), (5, 20480, 30720)])
+def test_icosphere_counts(sub, faces, edges):
+    m = M.icosphere(sub, 1.0)
+    assert m.num_faces == faces
+    assert m.num_edges == edges
+    assert len(m.points) == 10 * 4 ** sub + 2
+    np.testing.assert_allclose(np.linalg.norm(m.points, axis=1), 1.0, atol=1e-15)
+
+
+def test_outward_orientation_all_bodies():
+    for m in (M.icosphere(2, 1.0), M.ellipsoid(2, 2.0, 1.0, 0.5), M.superellipsoid(2, 1.0, 1.5, 0.8, 4.0)):
+        a, b, c = (m.points[m.faces[:, i]] for i in range(3))
+        n = np.cross(b - a, c - a)
+        assert np.all(np.einsum("ij,ij->i", n, a + b + c) > 0)
+
+
+def test_superellipsoid_surface():
+    m = M.superellipsoid(3, 1.0, 2.0, 0.5, 4.0)
+    s = np.sum(np.abs(m.points / np.array([1.0, 2.0, 0.5])) ** 4, axis=1)
+    np.testing.assert_allclose(s, 1.0, atol=1e-13)
+
+
+def test_nas_round_trip(tmp_path):
+    m = M.ellipsoid(2, 1.3, 0.7, 0.4)
+    p = M.write_nas(m, tmp_path / "b.nas")
+    r = M.read_nas(p)
+    np.testing.assert_array_equal(r.points, m.points)  # 17 significant digits: exact
+    np.testing.assert_array_equal(r.faces, m.faces)
+    text = p.read_text().splitlines()
+    assert any(t.startswith("GRID*") for t in text) and any(t.startswith("CTRIA3") for t in text)
+
+
+def test_mt19937_64_known_answer():
+    g = M._MT19937_64(5489)
+    assert g.next() == 14514284786278117030
+    for _ in range(9998):
+        g.next()
+    assert g.next() == 9981545732273789042  # 10000th output (C++ [rand.predef])
+
+
+def test_unit_disk_vector():
+    x = M.unit_disk_vector(2000, 0)
+    assert np.all(np.abs(x) <= 1.0)
+    assert abs(np.mean(np.abs(x) ** 2) - 0.5) < 0.03
+    np.testing.assert_array_equal(x, M.unit_disk_vector(2000, 0))
