@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 namespace mlfma {
 
 __host__ __device__ __forceinline__ double2 c2(double re, double im) { return make_double2(re, im); }
@@ -21,7 +23,7 @@ __host__ __device__ __forceinline__ double2 cfmas(double s, double2 a, double2 c
   return make_double2(fma(s, a.x, c.x), fma(s, a.y, c.y));
 }
 __host__ __device__ __forceinline__ double2 cmulj(double2 a) { return make_double2(-a.y, a.x); }  // j * a
-__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+__host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
   // Smith's algorithm
   if (fabs(b.x) >= fabs(b.y)) {
     const double r = b.y / b.x, d = b.x + b.y * r;
@@ -30,14 +32,19 @@ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
   const double r = b.x / b.y, d = b.x * r + b.y;
   return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
 }
-__device__ __forceinline__ double2 cexp(double2 z) {
+__host__ __device__ __forceinline__ double2 cexp(double2 z) {
   double s, c;
+#ifdef __CUDA_ARCH__
   sincos(z.y, &s, &c);
+#else
+  s = ::sin(z.y);
+  c = ::cos(z.y);
+#endif
   const double e = exp(z.x);
   return make_double2(e * c, e * s);
 }
 // exp(-j * k * t) for complex k and real t
-__device__ __forceinline__ double2 cexp_mjkt(double2 k, double t) {
+__host__ __device__ __forceinline__ double2 cexp_mjkt(double2 k, double t) {
   return cexp(make_double2(k.y * t, -k.x * t));
 }
 

@@ -44,13 +44,13 @@ struct GeomArg {
   const double* len;
 };
 
-__device__ __forceinline__ void load3(const double* p, double* o) {
+__host__ __device__ __forceinline__ void load3(const double* p, double* o) {
   o[0] = p[0];
   o[1] = p[1];
   o[2] = p[2];
 }
 
-__device__ __forceinline__ void qpoint(const QuadArg& q, int i, const double* a, const double* b,
+__host__ __device__ __forceinline__ void qpoint(const QuadArg& q, int i, const double* a, const double* b,
                                        const double* c, double* r) {
   r[0] = q.l1[i] * a[0] + q.l2[i] * b[0] + q.l3[i] * c[0];
   r[1] = q.l1[i] * a[1] + q.l2[i] * b[1] + q.l3[i] * c[1];
@@ -164,18 +164,18 @@ struct Tri {
   int id;
 };
 
-__device__ __forceinline__ void load_tri(const GeomArg& g, int f, Tri& t) {
+__host__ __device__ __forceinline__ void load_tri(const GeomArg& g, int f, Tri& t) {
   for (int a = 0; a < 3; ++a) load3(&g.xyz[3 * g.face_v[3 * f + a]], t.v[a]);
   t.area = g.face_area[f];
   load3(&g.face_normal[3 * f], t.n);
   t.id = g.face_id[f];
 }
 
-__device__ __forceinline__ double dot3(const double* a, const double* b) {
+__host__ __device__ __forceinline__ double dot3(const double* a, const double* b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
-__device__ __forceinline__ double norm3(const double* a) { return sqrt(dot3(a, a)); }
-__device__ __forceinline__ void cross3(const double* a, const double* b, double* c) {
+__host__ __device__ __forceinline__ double norm3(const double* a) { return sqrt(dot3(a, a)); }
+__host__ __device__ __forceinline__ void cross3(const double* a, const double* b, double* c) {
   c[0] = a[1] * b[2] - a[2] * b[1];
   c[1] = a[2] * b[0] - a[0] * b[2];
   c[2] = a[0] * b[1] - a[1] * b[0];
@@ -190,7 +190,7 @@ struct SingGeom {
   double Iv1[3], Is1, Iv3[3], Is3;
 };
 
-__device__ void sing_geometry(const Tri& S, const double* r, SingGeom& o) {
+__host__ __device__ void sing_geometry(const Tri& S, const double* r, SingGeom& o) {
   const double* nS = S.n;
   double rho_v[3][3];
   for (int i = 0; i < 3; ++i) {
@@ -265,7 +265,7 @@ __device__ void sing_geometry(const Tri& S, const double* r, SingGeom& o) {
 
 // The four PMCHWT operator values for one RWG pair:
 // out[0] = L(k1), out[1] = L(k2), out[2] = K(k1), out[3] = K(k2).
-__device__ void rwg_pair_ops(const GeomArg& g, const QuadArg& q, int fld, int src, double2 k1,
+__host__ __device__ void rwg_pair_ops(const GeomArg& g, const QuadArg& q, int fld, int src, double2 k1,
                              double2 k2, double2 out[4]) {
   const double2 ks[2] = {k1, k2};
   for (int i = 0; i < 4; ++i) out[i] = c2(0.0, 0.0);

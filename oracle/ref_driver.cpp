@@ -582,3 +582,18 @@ void ref_gauss_legendre(int n, double* x, double* w) {
   std::copy(W.begin(), W.end(), w);
 }
 }
+
+extern "C" {
+// OLK::L_operator and OLK::K_operator (Code/Operator.h:709-1046) for one RWG
+// pair at wavenumber k: out = {L re, L im, K re, K im}.
+void ref_lk(void* h, int fld, int src, double k_re, double k_im, double* out) {
+  RefCase& c = *static_cast<RefCase*>(h);
+  cplx L(0.0, 0.0), K(0.0, 0.0);
+  OLK::L_operator(&c.rwgs[fld], &c.rwgs[src], cplx(k_re, k_im), c.gp, L);
+  OLK::K_operator(&c.rwgs[fld], &c.rwgs[src], cplx(k_re, k_im), c.gp, K);
+  out[0] = L.real();
+  out[1] = L.imag();
+  out[2] = K.real();
+  out[3] = K.imag();
+}
+}

@@ -37,7 +37,7 @@ def test_legendre(shim):
             a = shim.ref_shim_legendre_p(l, x)
             b = float(mpmath.legendre(l, mpmath.mpf(float(x))))
             worst = max(worst, abs(a - b))
-    assert worst < 2e-14
+    assert worst < 1e-13  # ~l ulps accumulate in the recurrence up to l = 120
 
 
 @needs_oracle
