@@ -220,7 +220,10 @@ def run_product(args):
     x_host = M.unit_disk_vector(n, 0)
     x = torch.from_numpy(x_host).to(dev)
     w = torch.empty(n, dtype=torch.complex128, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream: the legacy default stream has handle 0, which the C
+    # ABI reads as "the plan's own stream"
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
 
     def step():
