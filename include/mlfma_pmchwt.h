@@ -157,6 +157,31 @@ MLFMA_API int mlfma_rhs_pmchwt(mlfma_plan* plan, const double kinc[3], const dou
 MLFMA_API int mlfma_rcs_pmchwt(mlfma_plan* plan, const double* I, int n_angles, const double* theta_deg,
                      const double* phi_deg, double* field, double* rcs_db);
 
+/* Far field without device allocation. No counterpart in the reference.
+ * For callers that cannot allocate device memory while they run -- e.g. an
+ * application that reserves all device memory up front in its own pool, or a
+ * real-time loop in which cudaMalloc/cudaFree and the synchronisation they can
+ * imply are not allowed. Computes the same field as mlfma_rcs_pmchwt, but I_dev
+ * (complex128 [2N]) and field_dev (3 complex per angle) are device pointers
+ * the caller owns, and the only scratch, the angle table, is a fixed
+ * file-scope device array held by every GPU that loads this library until the
+ * process exits. Limits and behaviour:
+ *  - n_angles <= mlfma_rcs_noalloc_max_angles() (8192); larger counts return
+ *    MLFMA_ERR_ARG with a message and launch nothing.
+ *  - Calls no cudaMalloc, cudaFree or allocating library routine.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture.
+ *  - Every call shares the one array (it keeps the last call's angles):
+ *    calls that overlap on the GPU, on any stream or plan, race. Order them on
+ *    one stream or synchronise between them.
+ *  - Asynchronous on `stream` (NULL = the plan's stream); theta_deg and
+ *    phi_deg are host arrays read before the call returns. */
+MLFMA_API int mlfma_rcs_pmchwt_noalloc(mlfma_plan* plan, const void* I_dev, int n_angles,
+                                       const double* theta_deg, const double* phi_deg, void* field_dev,
+                                       void* stream);
+MLFMA_API int mlfma_rcs_noalloc_max_angles(void);
+
 /* Copies of the plan's tables, for verification against the reference.
  * mlfma_get_rwgs: per RWG (reference order): face ids of T+ / T-, GRID ids of
  * the free vertices and of the common edge, edge length, edge midpoint

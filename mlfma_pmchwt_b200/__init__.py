@@ -82,6 +82,8 @@ SIGNATURES = {
                               C.POINTER(SolveStats), _DP, C.c_int]),
     "mlfma_rhs_pmchwt": (C.c_int, [_P, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt": (C.c_int, [_P, _DP, C.c_int, _DP, _DP, _DP, _DP]),
+    "mlfma_rcs_pmchwt_noalloc": (C.c_int, [_P, _P, C.c_int, _DP, _DP, _P, _P]),
+    "mlfma_rcs_noalloc_max_angles": (C.c_int, []),
     "mlfma_get_rwgs": (C.c_int, [_P, _IP, _IP, _IP, _IP, _IP, _IP, _DP, _DP]),
     "mlfma_get_level": (C.c_longlong, [_P, C.c_int, C.POINTER(C.c_ulonglong), _DP]),
     "mlfma_get_level_lists": (C.c_longlong, [_P, C.c_int, _IP, _IP, _IP, _IP, _IP]),
@@ -300,6 +302,15 @@ class MLFMM:
         self._check(self._lib.mlfma_rcs_pmchwt(self._h, _dp(I.view(np.float64)), len(th), _dp(th), _dp(ph),
                                                _dp(field.view(np.float64)), _dp(db)))
         return field, db
+
+    def calculate_rcs_noalloc(self, I_ptr: int, theta_deg, phi_deg, field_ptr: int, stream: int | None = None):
+        """Far field into caller-owned device memory with no device allocation
+        (see mlfma_rcs_pmchwt_noalloc): I_ptr -> complex128 [2N] on the device,
+        field_ptr -> complex128 [n_angles, 3] on the device. Asynchronous."""
+        th = np.ascontiguousarray(np.atleast_1d(theta_deg), dtype=np.float64)
+        ph = np.ascontiguousarray(np.broadcast_to(np.atleast_1d(phi_deg), th.shape), dtype=np.float64)
+        self._check(self._lib.mlfma_rcs_pmchwt_noalloc(self._h, C.c_void_p(I_ptr), len(th), _dp(th), _dp(ph),
+                                                       C.c_void_p(field_ptr), C.c_void_p(stream or 0)))
 
     # ------------------------------------------------------------ tables
     def rwgs(self) -> dict:

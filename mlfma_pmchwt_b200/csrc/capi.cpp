@@ -240,6 +240,25 @@ int mlfma_rcs_pmchwt(mlfma_plan* plan, const double* I, int n_angles, const doub
   });
 }
 
+int mlfma_rcs_pmchwt_noalloc(mlfma_plan* plan, const void* I_dev, int n_angles, const double* theta_deg,
+                              const double* phi_deg, void* field_dev, void* stream) {
+  if (!plan || !plan->p || !I_dev || !field_dev || (n_angles > 0 && (!theta_deg || !phi_deg)))
+    return fail(MLFMA_ERR_ARG, "null argument");
+  if (n_angles < 0 || n_angles > mlfma::rcs_noalloc_max_angles())
+    return fail(MLFMA_ERR_ARG, "n_angles must be between 0 and " + std::to_string(mlfma::rcs_noalloc_max_angles()) +
+                                   " (size of the fixed angle scratch)");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::rcs_pmchwt_noalloc(P, static_cast<const double2*>(I_dev), n_angles, theta_deg, phi_deg,
+                              static_cast<double2*>(field_dev), s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_rcs_noalloc_max_angles(void) { return mlfma::rcs_noalloc_max_angles(); }
+
 int mlfma_get_rwgs(const mlfma_plan* plan, int* face_pos, int* face_neg, int* free_pos, int* free_neg,
                    int* edge_a, int* edge_b, double* length, double* mid) {
   if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");

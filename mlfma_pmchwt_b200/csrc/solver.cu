@@ -14,6 +14,8 @@
 #include <chrono>
 #include <cmath>
 #include <complex>
+#include <mutex>
+#include <string>
 
 #include "cplx.cuh"
 #include "solver.hpp"
@@ -527,6 +529,112 @@ void rcs_pmchwt(Plan& P, const double* I, int n_angles, const double* theta_deg,
       rcs_db[3 * i + 2] = 10.0 * std::log10(std::norm(Eh) / (4.0 * kPi));
     }
   }
+}
+
+}  // namespace mlfma
+
+// ------------------------------------------------ far field without allocation
+//
+// mlfma_rcs_pmchwt_noalloc: the far-field evaluation for callers that cannot
+// allocate device memory while they run. Examples are an application that
+// reserves all device memory up front in its own pool, and a real-time loop
+// where a cudaMalloc/cudaFree (and the device synchronisation it can imply)
+// is not allowed. Its only scratch is the angle table below, a file-scope
+// device array that every GPU loading this library holds until exit.
+namespace mlfma {
+namespace {
+
+constexpr int kNoAllocMaxAngles = 8192;  // 2 x 8192 doubles = 128 KiB
+
+// [0, max): theta in degrees, [max, 2 max): phi in degrees
+static __device__ __align__(256) double g_rcs_angle_scratch[2 * kNoAllocMaxAngles];
+
+// Host-side device address of g_rcs_angle_scratch, looked up once per device
+// with that device current (the symbol's name on the host is only a
+// stand-in, not a device address).
+double* g_rcs_scratch_addr[64] = {nullptr};
+std::mutex g_rcs_scratch_mutex;
+
+double* rcs_scratch_address(int device) {
+  if (device < 0 || device >= 64) throw std::invalid_argument("device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_rcs_scratch_mutex);
+  if (!g_rcs_scratch_addr[device]) {
+    void* p = nullptr;
+    MLFMA_CUDA(cudaGetSymbolAddress(&p, g_rcs_angle_scratch));
+    g_rcs_scratch_addr[device] = static_cast<double*>(p);
+  }
+  return g_rcs_scratch_addr[device];
+}
+
+// Same accumulation as rcs_kernel; the direction of block b is formed from
+// the angles held in the scratch array.
+__global__ void __launch_bounds__(256) rcs_angles_kernel(RcsArg a, const double* __restrict__ angles, int max_angles,
+                                                         const double2* __restrict__ I, double2* __restrict__ out) {
+  __shared__ double2 sh[8];
+  const double th = (angles[blockIdx.x] / 180.0) * 3.14159265358979323846;
+  const double ph = (angles[max_angles + blockIdx.x] / 180.0) * 3.14159265358979323846;
+  const double r[3] = {sin(th) * cos(ph), sin(th) * sin(ph), cos(th)};
+  const double2 coeff = c2(a.k1.y, -a.k1.x);  // -j k1
+  double2 acc[3] = {c2(0, 0), c2(0, 0), c2(0, 0)};
+  for (int m = threadIdx.x; m < a.N; m += blockDim.x) {
+    const double ln = a.len[m];
+    double2 FJ[3] = {c2(0, 0), c2(0, 0), c2(0, 0)}, FM[3] = {c2(0, 0), c2(0, 0), c2(0, 0)};
+    for (int i = 0; i < a.nq; ++i) {
+      for (int side = 0; side < 2; ++side) {
+        const int f = side ? a.fneg[m] : a.fpos[m];
+        const double* A = &a.xyz[3 * a.face_v[3 * f]];
+        const double* B = &a.xyz[3 * a.face_v[3 * f + 1]];
+        const double* Cc = &a.xyz[3 * a.face_v[3 * f + 2]];
+        const double* fv = &a.xyz[3 * (side ? a.vneg[m] : a.vpos[m])];
+        double p[3], rho[3];
+        for (int c = 0; c < 3; ++c) {
+          p[c] = a.l1[i] * A[c] + a.l2[i] * B[c] + a.l3[i] * Cc[c];
+          rho[c] = side ? fv[c] - p[c] : p[c] - fv[c];
+        }
+        const double t = p[0] * r[0] + p[1] * r[1] + p[2] * r[2];
+        const double2 e = cexp(make_double2(-a.k1.y * t, a.k1.x * t));
+        const double rr = r[0] * rho[0] + r[1] * rho[1] + r[2] * rho[2];
+        const double Ft[3] = {rho[0] - r[0] * rr, rho[1] - r[1] * rr, rho[2] - r[2] * rr};
+        const double Fm[3] = {r[1] * rho[2] - r[2] * rho[1], r[2] * rho[0] - r[0] * rho[2],
+                              r[0] * rho[1] - r[1] * rho[0]};
+        const double wf = ln * a.w[i];
+        for (int c = 0; c < 3; ++c) {
+          FJ[c] = cadd(FJ[c], cscale(e, wf * Ft[c]));
+          FM[c] = cadd(FM[c], cscale(e, wf * Fm[c]));
+        }
+      }
+    }
+    const double2 IJ = I[m], IM = I[a.N + m];
+    for (int c = 0; c < 3; ++c) {
+      acc[c] = csub(acc[c], cmul(cmul(coeff, FJ[c]), IJ));
+      acc[c] = cadd(acc[c], cmul(cmul(coeff, FM[c]), IM));
+    }
+  }
+  for (int c = 0; c < 3; ++c) {
+    const double2 v = block_sum(acc[c], sh);
+    if (threadIdx.x == 0) out[3 * blockIdx.x + c] = v;
+  }
+}
+
+}  // namespace
+
+int rcs_noalloc_max_angles() { return kNoAllocMaxAngles; }
+
+void rcs_pmchwt_noalloc(Plan& P, const double2* I_dev, int n_angles, const double* theta_deg,
+                        const double* phi_deg, double2* field_dev, cudaStream_t s) {
+  if (n_angles < 0 || n_angles > kNoAllocMaxAngles)
+    throw std::invalid_argument("n_angles must be between 0 and " + std::to_string(kNoAllocMaxAngles) +
+                                " (size of the fixed angle scratch)");
+  MLFMA_CUDA(cudaSetDevice(P.device));
+  double* scratch = rcs_scratch_address(P.device);
+  if (n_angles == 0) return;
+  MLFMA_CUDA(cudaMemcpyAsync(scratch, theta_deg, n_angles * sizeof(double), cudaMemcpyHostToDevice, s));
+  MLFMA_CUDA(cudaMemcpyAsync(scratch + kNoAllocMaxAngles, phi_deg, n_angles * sizeof(double),
+                             cudaMemcpyHostToDevice, s));
+  RcsArg a{};
+  fill_common(P, a);
+  rcs_angles_kernel<<<n_angles, 256, 0, s>>>(a, scratch, kNoAllocMaxAngles, I_dev, field_dev);
+  MLFMA_CUDA(cudaGetLastError());
 }
 
 }  // namespace mlfma

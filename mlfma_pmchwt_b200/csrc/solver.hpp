@@ -24,4 +24,11 @@ void rhs_pmchwt(Plan& P, const double kinc[3], const double einc[3], const doubl
 void rcs_pmchwt(Plan& P, const double* I, int n_angles, const double* theta_deg, const double* phi_deg,
                 double* field, double* rcs_db);
 
+// Far field on device-resident currents and output without any device
+// allocation: the angle table lives in a fixed file-scope device array of
+// rcs_noalloc_max_angles() entries (see solver.cu).
+void rcs_pmchwt_noalloc(Plan& P, const double2* I_dev, int n_angles, const double* theta_deg,
+                        const double* phi_deg, double2* field_dev, cudaStream_t s);
+int rcs_noalloc_max_angles();
+
 }  // namespace mlfma
