@@ -43,6 +43,9 @@ def workload(args):
     if args.size == "full":
         return dict(name="sphere r=5 lambda, icosphere sub 6, 245,760 unknowns, eps_r 2.5-0.1j, leaf 0.25 lambda, "
                          "7-pt rule, FP64", sub=6, radius=5 * lam, eps=complex(2.5, -0.1), leaf=0.25)
+    if args.size == "mid":
+        return dict(name="sphere r=2.5 lambda, icosphere sub 5, 61,440 unknowns, eps_r 4, leaf 0.25 lambda, "
+                         "7-pt rule, FP64", sub=5, radius=2.5 * lam, eps=complex(4.0, 0.0), leaf=0.25)
     return dict(name="sphere r=1 m, icosphere sub 3, 3,840 unknowns, eps_r 4, leaf 0.25 lambda, 7-pt rule, FP64",
                 sub=3, radius=1.0, eps=complex(4.0, 0.0), leaf=0.25)
 
@@ -133,7 +136,8 @@ def stage_bytes(op) -> dict:
     inf = op.info
     L = op.max_level
     c16 = 16.0
-    b = {"aggregation": 0.0, "interpolation_up": 0.0, "translation_down": 0.0, "leaf_testing_near": 0.0}
+    b = {"aggregation": 0.0, "interpolation_up": 0.0, "translation": 0.0, "anterpolation_down": 0.0,
+         "leaf_testing_near": 0.0}
     for Ks in (inf.K_k1, inf.K_k2):
         Kl = Ks[L - 2]
         Bl = inf.boxes[L - 2]
@@ -143,10 +147,11 @@ def stage_bytes(op) -> dict:
             b["interpolation_up"] += inf.boxes[i + 1] * 6 * Ks[i + 1] * c16 + inf.boxes[i] * 6 * Ks[i] * c16
         for l in range(2, L + 1):
             i = l - 2
-            nvec = 316  # upper bound of the translation table rows at a level
-            b["translation_down"] += 2 * inf.boxes[i] * 6 * Ks[i] * c16 + min(nvec, 343) * Ks[i] * c16 * 0
+            # Sm read once, Bm written once
+            b["translation"] += 2 * inf.boxes[i] * 6 * Ks[i] * c16
             if l > 2:
-                b["translation_down"] += inf.boxes[i - 1] * 6 * Ks[i - 1] * c16
+                # parent Bm read once, child Bm read and written
+                b["anterpolation_down"] += inf.boxes[i - 1] * 6 * Ks[i - 1] * c16 + 2 * inf.boxes[i] * 6 * Ks[i] * c16
         b["leaf_testing_near"] += op.N * 3 * Kl * c16 + Bl * 6 * Kl * c16
     b["leaf_testing_near"] += inf.near_pairs * 3 * c16 + 4 * op.n * c16
     return b
@@ -229,6 +234,120 @@ def run_product(args):
     def step():
         op.apply_device(x.data_ptr(), w.data_ptr(), sp)
 
+    tune = op.autotune(3)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    # timed region: device time, max over ranks
+    op.profile(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    ms_local = e0.elapsed_time(e1)
+    stage_ms, napp = op.stage_times()
+    op.profile(False)
+    ms_total = allreduce_max(ms_local, world, dev)
+    ms_per_step = ms_total / args.steps
+    value = world * args.steps / (ms_total / 1000.0)
+
+    # end to end through the C ABI with pinned host buffers
+    xh = torch.from_numpy(x_host).pin_memory()
+    wh = torch.empty(n, dtype=torch.complex128).pin_memory()
+    xh_np, wh_np = xh.numpy(), wh.numpy()
+    for _ in range(2):
+        op._lib.mlfma_apply(op._h, n, xh_np.ctypes.data_as(_dp_t()), wh_np.ctypes.data_as(_dp_t()))
+    barrier(world)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        rc = op._lib.mlfma_apply(op._h, n, xh_np.ctypes.data_as(_dp_t()), wh_np.ctypes.data_as(_dp_t()))
+        if rc != 0:
+            raise RuntimeError(op._lib.mlfma_last_error().decode())
+    e2e_s = allreduce_max(time.perf_counter() - t, world, dev)
+    barrier(world)
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * 16,
+           "d2h_bytes_per_step": n * 16}
+
+    # roofline of the dominant stage (HBM-bound FP64 path)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    sb = stage_bytes(op)
+    per_apply_ms = {k: v / max(napp, 1) for k, v in stage_ms.items()}
+    dom = max(per_apply_ms, key=per_apply_ms.get)
+    achieved = sb[dom] / (per_apply_ms[dom] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": None,
+                "algorithmic_bytes": sb[dom],
+                "stage_ms_per_apply": {k: round(v, 4) for k, v in per_apply_ms.items()},
+                "matvec_bytes": sum(sb.values()),
+                "matvec_frac": round(sum(sb.values()) / (ms_per_step / 1000.0) / 1e9 / peak, 4)}
+
+    # solve of the plane-wave excitation (x-polarised, incident along -z) to
+    # 1e-3: flexible GMRES(50) with the near-field preconditioner, and the
+    # plain GMRES(50) of the reference for comparison (capped iterations)
+    solve = None
+    if args.solve_its > 0:
+        from mlfma_pmchwt_b200 import plane_wave
+        V = op.compute_v_pmchwt(*plane_wave(0.0, 0.0, 0.0))
+        xs, st = op.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
+                                  inner_its=args.inner_its)
+        solve = {"s_per_rhs": round(st["seconds"], 4), "iterations": st["iterations"],
+                 "converged": st["converged"], "rel_residual": st["rel_residual"], "restart": 50, "tol": 1e-3,
+                 "solver": f"FGMRES(50), right preconditioner = {args.inner_its} GMRES steps on the near field",
+                 "matvecs": st["matvecs"], "near_products": st["near_products"], "itr_max": args.solve_its}
+        if args.plain_its > 0:
+            xp, sp_ = op.matrix_solver(V, itr_max=args.plain_its, mr=50, tol_abs=1e-8, tol_rel=1e-3)
+            solve["plain_gmres"] = {"s": round(sp_["seconds"], 4), "iterations": sp_["iterations"],
+                                    "converged": sp_["converged"], "rel_residual": sp_["rel_residual"]}
+
+    line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / base["value"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": wl["name"], "parallelism": "openmp", "l2": "inputs larger than L2"},
+            "impl": "reference", "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_product(args):
+    import torch
+    from mlfma_pmchwt_b200 import MLFMM
+    from mlfma_pmchwt_b200 import mesh as M
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    wl = workload(args)
+    m = M.icosphere(wl["sub"], wl["radius"])
+    t0 = time.perf_counter()
+    op = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local)
+    setup_s = time.perf_counter() - t0
+    n = op.n
+    x_host = M.unit_disk_vector(n, 0)
+    x = torch.from_numpy(x_host).to(dev)
+    w = torch.empty(n, dtype=torch.complex128, device=dev)
+    # a dedicated stream: the legacy default stream has handle 0, which the C
+    # ABI reads as "the plan's own stream"
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+
+    def step():
+        op.apply_device(x.data_ptr(), w.data_ptr(), sp)
+
+    tune = op.autotune(3)
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize(dev)
@@ -301,9 +420,11 @@ def run_product(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": wl["name"], "unknowns": n, "max_level": op.max_level,
                        "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
-                       "setup_s": round(setup_s, 2), "device_bytes": op.info.bytes_device},
+                       "setup_s": round(setup_s, 2), "device_bytes": op.info.bytes_device,
+                       "tuning": {"m2l.variant": tune["m2l.variant"],
+                                  "variant_ms": [round(v, 4) for v in tune["variant_ms"]]}},
             "e2e": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in e2e.items()},
-            "gpu_launches": args.steps * (2 * (1 + 2 * (op.max_level - 2) + 1) + 1),
+            "gpu_launches": args.steps * (2 * (1 + 3 * (op.max_level - 2) + 1) + 1),
             "roofline": roofline, "clocks": clk}
     if solve:
         line["solve"] = solve
@@ -331,8 +452,10 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["product", "reference"], default="product")
-    ap.add_argument("--size", choices=["full", "small"], default="full")
-    ap.add_argument("--solve-its", type=int, default=300)
+    ap.add_argument("--size", choices=["full", "mid", "small"], default="full")
+    ap.add_argument("--solve-its", type=int, default=1000, help="outer iteration cap of the solve")
+    ap.add_argument("--inner-its", type=int, default=16, help="near-field GMRES steps per preconditioning")
+    ap.add_argument("--plain-its", type=int, default=300, help="iteration cap of the plain GMRES comparison")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference matvecs to time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)

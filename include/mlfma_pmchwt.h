@@ -64,6 +64,9 @@ typedef struct {
   int precision;               /* MLFMA_PREC_FP64 */
   int device;                  /* CUDA device ordinal */
   int verbose;                 /* print setup summary to stderr */
+  int tf_complex_argument;     /* 0 (default): transfer factors with h2_l(|kR|) as the reference
+                                  (Code/AlgoMLFMM.h:262-265); 1: h2_l(kR) with complex kR, a
+                                  departure from the reference for lossy media */
 } mlfma_params;
 
 #define MLFMA_PREC_FP64 0
@@ -91,6 +94,7 @@ typedef struct {
   double rel_residual;         /* last true residual ||b - A x|| / ||b|| */
   double seconds;              /* device time of the solve */
   int history_len;             /* entries written to history */
+  int near_products;           /* near-field-only products spent in the preconditioner */
 } mlfma_solve_stats;
 
 MLFMA_API void mlfma_default_params(mlfma_params* p);
@@ -125,10 +129,20 @@ MLFMA_API int mlfma_apply_device(mlfma_plan* plan, int n, const void* x_dev, voi
 /* Stage timing (no counterpart in the reference, whose timers are
  * std::chrono prints): with on != 0 every apply records CUDA events on its
  * stream between stage groups; mlfma_profile_read sums them since the last
- * read into stage_ms[4] = {aggregation, interpolation up, translation +
+ * read into stage_ms[5] = {aggregation, interpolation up, translation,
  * anterpolation down, leaf testing + near field} and the number of applies. */
 MLFMA_API int mlfma_profile(mlfma_plan* plan, int on);
 MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applies);
+
+/* Kernel variants of a plan (no counterpart in the reference). key
+ * "m2l.variant": 0 = one thread per (box, direction) over the interaction
+ * list, 1 = sibling-group tiles staging the shared sources in shared memory
+ * (default). mlfma_autotune times each variant over `applies` applies of the
+ * plan's own operator (device vectors owned by the plan) and keeps the
+ * fastest; variant_ms receives the per-apply time of each (may be NULL). */
+MLFMA_API int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value);
+MLFMA_API int mlfma_get_tuning(const mlfma_plan* plan, const char* key);
+MLFMA_API int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms);
 
 /* Restarted GMRES(mr) with the operator -- replaces MGMRES::mgmres
  * (Code/GMRES.h:65-217) driven by MLFMM::matrix_solver (Code/MLFMM.cpp:186).
@@ -141,6 +155,21 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
 MLFMA_API int mlfma_gmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr,
                 double tol_abs, double tol_rel, mlfma_solve_stats* stats, double* history,
                 int history_cap);
+
+/* Flexible GMRES(mr) with a near-field preconditioner. No direct
+ * counterpart in the reference, whose only solvers are MGMRES::mgmres and
+ * CGS (Code/CGS.h). Arguments, stopping rule, true residual per cycle and
+ * divergence abort are those of mlfma_gmres. The right preconditioner is
+ * inner_its GMRES steps from zero on the near-field matrix alone (the Z_near
+ * rows of Code/Zmartix.h:541-643); inner_its = 0 reduces to plain GMRES.
+ * itr_max counts outer steps; stats->near_products counts inner products. */
+MLFMA_API int mlfma_fgmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr,
+                           double tol_abs, double tol_rel, int inner_its, mlfma_solve_stats* stats,
+                           double* history, int history_cap);
+
+/* w = Z_near x on device vectors: the near-field rows alone (the product of
+ * Code/MLFMM.cpp:353-366 without the far field). Asynchronous on stream. */
+MLFMA_API int mlfma_apply_near_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream);
 
 /* Plane-wave excitation vector V (complex128 [2N]) -- RHS::computeV_PMCHWT
  * (Code/Vm.h:150-203) with the incident unit vectors of EMSource::initPW

@@ -45,7 +45,8 @@ class _MeshStruct(C.Structure):
 class Params(C.Structure):
     _fields_ = [("freq_hz", C.c_double), ("eps_r_re", C.c_double), ("eps_r_im", C.c_double),
                 ("mu_r_re", C.c_double), ("mu_r_im", C.c_double), ("leaf_coeff", C.c_double),
-                ("gauss_points", C.c_int), ("precision", C.c_int), ("device", C.c_int), ("verbose", C.c_int)]
+                ("gauss_points", C.c_int), ("precision", C.c_int), ("device", C.c_int), ("verbose", C.c_int),
+                ("tf_complex_argument", C.c_int)]
 
 
 class Info(C.Structure):
@@ -59,7 +60,8 @@ class Info(C.Structure):
 
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("restarts", C.c_int), ("matvecs", C.c_int), ("converged", C.c_int),
-                ("rel_residual", C.c_double), ("seconds", C.c_double), ("history_len", C.c_int)]
+                ("rel_residual", C.c_double), ("seconds", C.c_double), ("history_len", C.c_int),
+                ("near_products", C.c_int)]
 
 
 # Exported symbols with their ctypes signatures (mirrors include/mlfma_pmchwt.h).
@@ -78,8 +80,14 @@ SIGNATURES = {
     "mlfma_apply_device": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mlfma_profile": (C.c_int, [_P, C.c_int]),
     "mlfma_profile_read": (C.c_int, [_P, _DP, C.POINTER(C.c_int)]),
+    "mlfma_set_tuning": (C.c_int, [_P, C.c_char_p, C.c_int]),
+    "mlfma_get_tuning": (C.c_int, [_P, C.c_char_p]),
+    "mlfma_autotune": (C.c_int, [_P, C.c_int, _DP]),
     "mlfma_gmres": (C.c_int, [_P, C.c_int, _DP, _DP, C.c_int, C.c_int, C.c_double, C.c_double,
                               C.POINTER(SolveStats), _DP, C.c_int]),
+    "mlfma_fgmres": (C.c_int, [_P, C.c_int, _DP, _DP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                               C.POINTER(SolveStats), _DP, C.c_int]),
+    "mlfma_apply_near_device": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mlfma_rhs_pmchwt": (C.c_int, [_P, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt": (C.c_int, [_P, _DP, C.c_int, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt_noalloc": (C.c_int, [_P, _P, C.c_int, _DP, _DP, _P, _P]),
@@ -169,7 +177,7 @@ class MLFMM:
 
     def __init__(self, mesh: Mesh | None = None, *, nas_path: str | None = None, freq: float = 3.0e8,
                  eps_r: complex = 4.0, mu_r: complex = 1.0, leaf_coeff: float = 0.3, gauss_points: int = 7,
-                 device: int = 0, verbose: bool = False):
+                 device: int = 0, verbose: bool = False, tf_complex_argument: bool = False):
         self._lib = load_library()
         prm = Params()
         self._lib.mlfma_default_params(C.byref(prm))
@@ -177,6 +185,7 @@ class MLFMM:
         prm.freq_hz, prm.eps_r_re, prm.eps_r_im = freq, eps_r.real, eps_r.imag
         prm.mu_r_re, prm.mu_r_im = mu_r.real, mu_r.imag
         prm.leaf_coeff, prm.gauss_points, prm.device, prm.verbose = leaf_coeff, gauss_points, device, int(verbose)
+        prm.tf_complex_argument = int(tf_complex_argument)
         self.params = prm
         h = _P()
         if nas_path is not None:
@@ -255,7 +264,19 @@ class MLFMM:
         self._check(self._lib.mlfma_apply_device(self._h, self.n, C.c_void_p(x_ptr), C.c_void_p(w_ptr),
                                                  C.c_void_p(stream or 0)))
 
-    STAGES = ("aggregation", "interpolation_up", "translation_down", "leaf_testing_near")
+    def set_tuning(self, key: str, value: int):
+        self._check(self._lib.mlfma_set_tuning(self._h, key.encode(), int(value)))
+
+    def get_tuning(self, key: str) -> int:
+        return self._check(self._lib.mlfma_get_tuning(self._h, key.encode()))
+
+    def autotune(self, applies: int = 3) -> dict:
+        """Times each m2l variant on this plan and keeps the fastest."""
+        ms = np.zeros(2)
+        self._check(self._lib.mlfma_autotune(self._h, int(applies), _dp(ms)))
+        return {"m2l.variant": self.get_tuning("m2l.variant"), "variant_ms": ms.tolist()}
+
+    STAGES = ("aggregation", "interpolation_up", "translation", "anterpolation_down", "leaf_testing_near")
 
     def profile(self, on: bool = True):
         """Record per-stage CUDA events on every apply (see stage_times)."""
@@ -263,28 +284,39 @@ class MLFMM:
 
     def stage_times(self):
         """Summed stage times (ms) since the last call and the apply count."""
-        ms = np.zeros(4)
+        ms = np.zeros(len(self.STAGES))
         n = C.c_int(0)
         self._check(self._lib.mlfma_profile_read(self._h, _dp(ms), C.byref(n)))
         return dict(zip(self.STAGES, ms)), n.value
 
     def matrix_solver(self, rhs, x0=None, itr_max: int | None = None, mr: int = 50, tol_abs: float = 1e-8,
-                      tol_rel: float = 1e-4):
+                      tol_rel: float = 1e-4, inner_its: int | None = None):
         """Restarted GMRES(mr) (MGMRES::mgmres with MLFMM::matrix_solver's
         arguments, Code/RCS.h:364-375 defaults: itr_max = 2N, mr = 50,
-        tol_abs 1e-8, tol_rel 1e-4). Returns (x, stats dict)."""
+        tol_abs 1e-8, tol_rel 1e-4). With inner_its (>= 0) the solve is
+        flexible GMRES preconditioned by inner_its near-field GMRES steps
+        (mlfma_fgmres). Returns (x, stats dict)."""
         b = _c128(rhs)
         x = np.zeros(self.n, dtype=np.complex128) if x0 is None else _c128(x0).copy()
         itr_max = self.n if itr_max is None else int(itr_max)
         st = SolveStats()
         hist = np.zeros(max(itr_max, 1), dtype=np.float64)
-        rc = self._lib.mlfma_gmres(self._h, self.n, _dp(x.view(np.float64)), _dp(b.view(np.float64)), itr_max, mr,
-                                   tol_abs, tol_rel, C.byref(st), _dp(hist), len(hist))
+        if inner_its is None:
+            rc = self._lib.mlfma_gmres(self._h, self.n, _dp(x.view(np.float64)), _dp(b.view(np.float64)), itr_max,
+                                       mr, tol_abs, tol_rel, C.byref(st), _dp(hist), len(hist))
+        else:
+            rc = self._lib.mlfma_fgmres(self._h, self.n, _dp(x.view(np.float64)), _dp(b.view(np.float64)), itr_max,
+                                        mr, tol_abs, tol_rel, int(inner_its), C.byref(st), _dp(hist), len(hist))
         self._check(rc)
         stats = dict(iterations=st.iterations, restarts=st.restarts, matvecs=st.matvecs,
                      converged=bool(st.converged), rel_residual=st.rel_residual, seconds=st.seconds,
-                     history=hist[: st.history_len].copy())
+                     near_products=st.near_products, history=hist[: st.history_len].copy())
         return x, stats
+
+    def apply_near_device(self, x_ptr: int, w_ptr: int, stream: int | None = None):
+        """w = Z_near x on device pointers (the near-field rows alone)."""
+        self._check(self._lib.mlfma_apply_near_device(self._h, self.n, C.c_void_p(x_ptr), C.c_void_p(w_ptr),
+                                                      C.c_void_p(stream or 0)))
 
     def compute_v_pmchwt(self, kinc, einc, hinc) -> np.ndarray:
         V = np.empty(self.n, dtype=np.complex128)

@@ -53,6 +53,7 @@ mlfma::PlanParams to_params(const mlfma_params* p) {
   q.gauss = p->gauss_points;
   q.device = p->device;
   q.verbose = p->verbose;
+  q.tf_complex_argument = p->tf_complex_argument;
   return q;
 }
 
@@ -194,6 +195,67 @@ int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applies) {
   });
 }
 
+int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value) {
+  if (!plan || !plan->p || !key) return fail(MLFMA_ERR_ARG, "null argument");
+  const std::string k(key);
+  if (k == "m2l.variant") {
+    if (value < 0 || value > 1) return fail(MLFMA_ERR_ARG, "m2l.variant must be 0 or 1");
+    plan->p->tuning.m2l_variant = value;
+    return MLFMA_OK;
+  }
+  if (k == "l2l.variant") {
+    if (value < 0 || value > 1) return fail(MLFMA_ERR_ARG, "l2l.variant must be 0 or 1");
+    plan->p->tuning.l2l_variant = value;
+    return MLFMA_OK;
+  }
+  return fail(MLFMA_ERR_ARG, "unknown tuning key: " + k);
+}
+
+int mlfma_get_tuning(const mlfma_plan* plan, const char* key) {
+  if (!plan || !plan->p || !key) return fail(MLFMA_ERR_ARG, "null argument");
+  if (std::string(key) == "m2l.variant") return plan->p->tuning.m2l_variant;
+  if (std::string(key) == "l2l.variant") return plan->p->tuning.l2l_variant;
+  return fail(MLFMA_ERR_ARG, std::string("unknown tuning key: ") + key);
+}
+
+int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
+  if (!plan || !plan->p || applies <= 0) return fail(MLFMA_ERR_ARG, "null plan or applies <= 0");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    cudaEvent_t e0, e1;
+    MLFMA_CUDA(cudaEventCreate(&e0));
+    MLFMA_CUDA(cudaEventCreate(&e1));
+    MLFMA_CUDA(cudaMemsetAsync(P.d_x, 0, 2 * static_cast<size_t>(P.N) * sizeof(double2), P.stream));
+    const bool prof = P.prof.on;
+    P.prof.on = false;
+    double best = 1e300;
+    int best_v = P.tuning.m2l_variant;
+    for (int v = 0; v <= 1; ++v) {
+      P.tuning.m2l_variant = v;
+      mlfma::apply_device(P, P.d_x, P.d_w, P.stream);  // warm-up
+      MLFMA_CUDA(cudaEventRecord(e0, P.stream));
+      for (int i = 0; i < applies; ++i) mlfma::apply_device(P, P.d_x, P.d_w, P.stream);
+      MLFMA_CUDA(cudaEventRecord(e1, P.stream));
+      MLFMA_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      MLFMA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      const double per = ms / applies;
+      if (variant_ms) variant_ms[v] = per;
+      if (per < best) {
+        best = per;
+        best_v = v;
+      }
+    }
+    P.tuning.m2l_variant = best_v;
+    P.prof.on = prof;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return MLFMA_OK;
+  });
+}
+
 int mlfma_gmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr, double tol_abs,
                 double tol_rel, mlfma_solve_stats* stats, double* history, int history_cap) {
   if (!plan || !plan->p || !x || !rhs) return fail(MLFMA_ERR_ARG, "null argument");
@@ -212,10 +274,52 @@ int mlfma_gmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_m
       stats->rel_residual = st.rel_residual;
       stats->seconds = st.seconds;
       stats->history_len = static_cast<int>(std::min<size_t>(hist.size(), history ? history_cap : 0));
+      stats->near_products = 0;
     }
     if (history)
       for (int i = 0; i < history_cap && i < static_cast<int>(hist.size()); ++i) history[i] = hist[i];
     return ok ? MLFMA_OK : MLFMA_ERR_NOT_CONVERGED;
+  });
+}
+
+int mlfma_fgmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr, double tol_abs,
+                 double tol_rel, int inner_its, mlfma_solve_stats* stats, double* history, int history_cap) {
+  if (!plan || !plan->p || !x || !rhs) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (mr <= 0 || mr > 63 || itr_max < 0 || inner_its < 0 || inner_its > 63)
+    return fail(MLFMA_ERR_ARG, "need 1 <= mr <= 63, 0 <= inner_its <= 63, itr_max >= 0");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::SolveStats st;
+    std::vector<double> hist;
+    const bool ok = mlfma::fgmres_solve(*plan->p, x, rhs, itr_max, mr, tol_abs, tol_rel, inner_its, st, hist);
+    if (stats) {
+      stats->iterations = st.iterations;
+      stats->restarts = st.restarts;
+      stats->matvecs = st.matvecs;
+      stats->converged = ok ? 1 : 0;
+      stats->rel_residual = st.rel_residual;
+      stats->seconds = st.seconds;
+      stats->history_len = static_cast<int>(std::min<size_t>(hist.size(), history ? history_cap : 0));
+      stats->near_products = st.near_products;
+    }
+    if (history)
+      for (int i = 0; i < history_cap && i < static_cast<int>(hist.size()); ++i) history[i] = hist[i];
+    return ok ? MLFMA_OK : MLFMA_ERR_NOT_CONVERGED;
+  });
+}
+
+int mlfma_apply_near_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream) {
+  if (!plan || !plan->p || !x_dev || !w_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (x_dev == w_dev) return fail(MLFMA_ERR_ARG, "x and w must not alias");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::near_apply(P, static_cast<const double2*>(x_dev), static_cast<double2*>(w_dev), s);
+    return MLFMA_OK;
   });
 }
 

@@ -495,6 +495,15 @@ void hankel2_array(int L, double x, std::vector<cplx>& h2) {
   for (int l = 0; l <= L; ++l) h2[l] = cplx(sph_j(l, x), -sph_y(l, x));
 }
 
+void hankel2_array_complex(int L, cplx z, std::vector<cplx>& h2) {
+  h2.resize(L + 1);
+  const cplx I(0.0, 1.0);
+  const cplx e = std::exp(-I * z);
+  h2[0] = I * e / z;
+  if (L >= 1) h2[1] = e * (I / (z * z) - 1.0 / z);
+  for (int l = 1; l < L; ++l) h2[l + 1] = (2.0 * l + 1.0) / z * h2[l] - h2[l - 1];
+}
+
 // Code/OverloadAlgo.h:254-288: Newton on P_n from cos(pi (i+0.75)/(n+0.5)),
 // |dx| < 1e-10, at most 100 steps; nodes stored as -root / +root.
 void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {

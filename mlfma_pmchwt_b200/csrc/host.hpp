@@ -103,6 +103,9 @@ double legendre_dp(int l, double x);
 double sph_j(int n, double x);
 double sph_y(int n, double x);
 void hankel2_array(int L, double x, std::vector<cplx>& h2);
+// h2_l(z), l = 0..L, for complex z by the upward recurrence from
+// h2_0 = i e^{-iz}/z and h2_1 = e^{-iz} (i/z^2 - 1/z).
+void hankel2_array_complex(int L, cplx z, std::vector<cplx>& h2);
 void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
 
 // Triangle quadrature (Code/GaussPoints.cpp, Dunavant rules, weights sum to 1/2).

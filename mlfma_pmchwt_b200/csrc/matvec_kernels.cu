@@ -5,14 +5,14 @@
 //
 //   agg      leaf aggregation           Code/ProcessMLFMM.h:33-56   (mexp)
 //   up       interpolation + shift up   Code/ProcessMLFMM.h:61-107  (m2m)
-//   down     translation over the interaction list plus the parent's
-//            anterpolated, shifted incoming pattern
-//                                       Code/ProcessMLFMM.h:112-147 (m2l)
-//                                       Code/ProcessMLFMM.h:152-202 (l2l)
+//   m2l      translation over the interaction list   Code/ProcessMLFMM.h:112-147
+//   l2l      the parent's incoming pattern, shifted and anterpolated onto
+//            the child grid, added                    Code/ProcessMLFMM.h:152-202
 //   leaf_out receive-pattern testing of both media and the near-field rows,
 //            written once per unknown   Code/MLFMM.cpp:285-366
-// No stage accumulates into memory written by another launch of the same
-// matvec, so no clearing pass (Code/ProcessMLFMM.h:14-28) is needed.
+// Every stage writes its output before anything accumulates into it (l2l adds
+// onto the Bm that m2l of the same level has just written), so no clearing
+// pass (Code/ProcessMLFMM.h:14-28) is needed.
 #include "cplx.cuh"
 #include "plan.hpp"
 
@@ -62,9 +62,14 @@ struct UpArg {
   int Kp, nphp, Kc, nphc;
 };
 
+// One thread per (parent box, parent direction, component): the 9-tap
+// separable interpolation of each child's pattern, times the child's shift
+// phase, summed over the children. One component per thread keeps the
+// register count low enough for the occupancy this gather needs.
 __global__ void __launch_bounds__(kThreads) up_kernel(UpArg a) {
   const int kk = blockIdx.y * blockDim.x + threadIdx.x;
   const int b = blockIdx.x;
+  const int c = blockIdx.z;
   if (kk >= a.Kp) return;
   const int t = kk / a.nphp, p = kk - t * a.nphp;
   int ti[3], pi[3];
@@ -76,30 +81,22 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg a) {
     pi[i] = a.pidx[3 * p + i];
     wp[i] = a.lp[3 * p + i];
   }
-  double2 acc[6];
-#pragma unroll
-  for (int c = 0; c < 6; ++c) acc[c] = c2(0.0, 0.0);
+  double2 acc = c2(0.0, 0.0);
   const int c1 = a.child_begin[b + 1];
   for (int ch = a.child_begin[b]; ch < c1; ++ch) {
     const double2 e = a.ph_up[a.octant[ch] * a.Kp + kk];
-    const double2* src = a.Sc + static_cast<size_t>(ch) * 6 * a.Kc;
+    const double2* sc = a.Sc + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
+    double2 v = c2(0.0, 0.0);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      const double2* sc = src + static_cast<size_t>(c) * a.Kc;
-      double2 v = c2(0.0, 0.0);
+    for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) v = cfmas(wt[i] * wp[j], sc[ti[i] + pi[j]], v);
-      acc[c] = cfma(e, v, acc[c]);
-    }
+      for (int j = 0; j < 3; ++j) v = cfmas(wt[i] * wp[j], __ldg(sc + ti[i] + pi[j]), v);
+    acc = cfma(e, v, acc);
   }
-  double2* out = a.Sp + static_cast<size_t>(b) * 6 * a.Kp + kk;
-#pragma unroll
-  for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * a.Kp] = acc[c];
+  a.Sp[(static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
 }
 
-struct DownArg {
+struct M2lArg {
   const double2* S;     // this level's aggregated patterns
   double2* Bm;          // this level's incoming patterns (written)
   const int* far_ptr;
@@ -108,18 +105,12 @@ struct DownArg {
   const int* off2vec;
   const double2* tfw;
   int K;
-  // parent contribution (null Bp at the top level)
-  const double2* Bp;
-  const int* parent;
-  const int* octant;
-  const double2* ph_dn;  // parent level table [8][Kp]
-  const int* tr_ptr;
-  const int* tr_kp;
-  const double* tr_w;
-  int Kp;
 };
 
-__global__ void __launch_bounds__(kThreads) down_kernel(DownArg a) {
+// Translation (m2l): one thread per (box, direction); the 6 components of
+// each interaction-list source are applied with one transfer-factor load.
+// Writes Bm (no accumulation into an earlier value).
+__global__ void __launch_bounds__(kThreads) m2l_kernel(M2lArg a) {
   const int kk = blockIdx.y * blockDim.x + threadIdx.x;
   const int b = blockIdx.x;
   if (kk >= a.K) return;
@@ -134,21 +125,177 @@ __global__ void __launch_bounds__(kThreads) down_kernel(DownArg a) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) acc[c] = cfma(tf, src[static_cast<size_t>(c) * a.K], acc[c]);
   }
-  if (a.Bp) {
-    const int P = a.parent[b];
-    const double2* ph = a.ph_dn + a.octant[b] * a.Kp;
-    const double2* bp = a.Bp + static_cast<size_t>(P) * 6 * a.Kp;
-    const int t1 = a.tr_ptr[kk + 1];
-    for (int e = a.tr_ptr[kk]; e < t1; ++e) {
-      const int kp = a.tr_kp[e];
-      const double2 f = cscale(ph[kp], a.tr_w[e]);
-#pragma unroll
-      for (int c = 0; c < 6; ++c) acc[c] = cfma(f, bp[static_cast<size_t>(c) * a.Kp + kp], acc[c]);
-    }
-  }
   double2* out = a.Bm + static_cast<size_t>(b) * 6 * a.K + kk;
 #pragma unroll
   for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * a.K] = acc[c];
+}
+
+struct M2lTileArg {
+  const double2* S;
+  double2* Bm;
+  const int* child_begin;  // parent level: range of children (the targets)
+  const int* usrc_ptr;     // per parent: union of its children's interaction sources
+  const int* usrc;
+  const int* coord;        // [3 * B] integer box coordinates at this level
+  const int* off2vec;
+  const double2* tfw;
+  int K;
+};
+
+constexpr int kTileDirs = 32;   // directions per CTA (one per lane)
+constexpr int kTileWarps = 8;   // one warp per child slot of the parent
+constexpr int kTileBatch = 14;  // sources staged per round (static shared memory < 48 KB)
+
+// Translation by sibling groups: one CTA per (parent box, 32-direction
+// chunk), one warp per child. The union of the children's interaction
+// sources (children of the parent's 27-neighbourhood) is staged through
+// shared memory in batches, so each source pattern crosses L2 once per
+// sibling group instead of once per target. Each warp then applies the
+// sources that interact with its child (Chebyshev distance >= 2 in box
+// units), in the same ascending source order as m2l_kernel.
+__global__ void __launch_bounds__(kTileDirs * kTileWarps) m2l_tile_kernel(M2lTileArg a) {
+  __shared__ double2 sS[kTileBatch][6][kTileDirs];
+  __shared__ int sSrc[kTileBatch][4];  // x, y, z, box
+  __shared__ int sVec[343];
+  const int P = blockIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int kk = blockIdx.y * kTileDirs + lane;
+  for (int i = threadIdx.x; i < 343; i += blockDim.x) sVec[i] = a.off2vec[i];
+  const int c0 = a.child_begin[P], nc = a.child_begin[P + 1] - c0;
+  const int t = c0 + w;
+  const bool active = w < nc;
+  int tx = 0, ty = 0, tz = 0;
+  if (active) {
+    tx = a.coord[3 * t];
+    ty = a.coord[3 * t + 1];
+    tz = a.coord[3 * t + 2];
+  }
+  double2 acc[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) acc[c] = c2(0.0, 0.0);
+  const int u0 = a.usrc_ptr[P], nu = a.usrc_ptr[P + 1] - u0;
+  for (int base = 0; base < nu; base += kTileBatch) {
+    const int nb = min(kTileBatch, nu - base);
+    __syncthreads();
+    if (threadIdx.x < nb) {
+      const int sb = a.usrc[u0 + base + threadIdx.x];
+      sSrc[threadIdx.x][0] = a.coord[3 * sb];
+      sSrc[threadIdx.x][1] = a.coord[3 * sb + 1];
+      sSrc[threadIdx.x][2] = a.coord[3 * sb + 2];
+      sSrc[threadIdx.x][3] = sb;
+    }
+    // stage nb sources x 6 components x 32 directions (one 512-byte row per warp load)
+    for (int row = w; row < nb * 6; row += kTileWarps) {
+      const int j = row / 6, c = row - 6 * j;
+      const int sb = a.usrc[u0 + base + j];
+      sS[j][c][lane] = kk < a.K ? a.S[(static_cast<size_t>(sb) * 6 + c) * a.K + kk] : c2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (active && kk < a.K) {
+      for (int j = 0; j < nb; ++j) {
+        const int dx = tx - sSrc[j][0], dy = ty - sSrc[j][1], dz = tz - sSrc[j][2];
+        if (max(abs(dx), max(abs(dy), abs(dz))) < 2) continue;  // near: not translated
+        const int v = sVec[(dx + 3) * 49 + (dy + 3) * 7 + (dz + 3)];
+        const double2 tf = __ldg(a.tfw + static_cast<size_t>(v) * a.K + kk);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc[c] = cfma(tf, sS[j][c][lane], acc[c]);
+      }
+    }
+  }
+  if (active && kk < a.K) {
+    double2* out = a.Bm + static_cast<size_t>(t) * 6 * a.K + kk;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * a.K] = acc[c];
+  }
+}
+
+struct L2lArg {
+  double2* Bm;           // child level (accumulated into)
+  const double2* Bp;     // parent level
+  const int* parent;     // of child boxes
+  const int* octant;     // of child boxes
+  const double2* ph_dn;  // parent level table [8][Kp]
+  const int* tr_ptr;     // child direction -> (parent direction, weight)
+  const int* tr_kp;
+  const double* tr_w;
+  int K, Kp;
+};
+
+// Anterpolation (l2l): one thread per (child box, child direction,
+// component) adds the parent's incoming pattern, shifted to the child centre
+// and interpolated transposed onto the child grid.
+__global__ void __launch_bounds__(kThreads) l2l_kernel(L2lArg a) {
+  const int kk = blockIdx.y * blockDim.x + threadIdx.x;
+  const int b = blockIdx.x;
+  const int c = blockIdx.z;
+  if (kk >= a.K) return;
+  const double2* ph = a.ph_dn + a.octant[b] * a.Kp;
+  const double2* bp = a.Bp + (static_cast<size_t>(a.parent[b]) * 6 + c) * a.Kp;
+  double2 acc = c2(0.0, 0.0);
+  const int t1 = a.tr_ptr[kk + 1];
+  for (int e = a.tr_ptr[kk]; e < t1; ++e) {
+    const int kp = __ldg(a.tr_kp + e);
+    acc = cfma(cscale(__ldg(ph + kp), __ldg(a.tr_w + e)), __ldg(bp + kp), acc);
+  }
+  double2* out = a.Bm + (static_cast<size_t>(b) * 6 + c) * a.K + kk;
+  *out = cadd(*out, acc);
+}
+
+struct L2lSepArg {
+  double2* Bm;           // child level (accumulated into)
+  const double2* Bp;     // parent level
+  const int* parent;     // of child boxes
+  const int* octant;     // of child boxes
+  const double2* ph_dn;  // parent level table [8][Kp]
+  const int* th_ptr;     // child theta row -> (parent theta row, Lagrange weight)
+  const int* th_src;
+  const double* th_w;
+  const int* ph_ptr;     // child phi column -> (parent phi column, Lagrange weight)
+  const int* ph_src;
+  const double* ph_w;
+  int ntc, npc, ntp, npp;
+};
+
+constexpr int kL2lRows = 8;        // child theta rows per band at most
+constexpr int kL2lBand = 2944;     // band entries in shared memory (46 KiB)
+constexpr int kL2lMaxPhi = kL2lBand;
+
+// Anterpolation (l2l), separable: the parent's incoming pattern is shifted to
+// the child centre, then spread onto the child grid by the transposed
+// theta interpolation (into a shared-memory band of child rows x parent phi
+// columns) and the transposed phi interpolation. One CTA per (child box,
+// component); the reference's 9-tap weight of a (parent, child) direction
+// pair is the product of the two 1-D weights used here (Code/AlgoMLFMM.h:347-351).
+__global__ void __launch_bounds__(256) l2l_sep_kernel(L2lSepArg a) {
+  __shared__ double2 band[kL2lBand];
+  const int b = blockIdx.x, c = blockIdx.y;
+  const int band_rows = max(1, min(kL2lRows, kL2lBand / a.npp));
+  const int Kp = a.ntp * a.npp, Kc = a.ntc * a.npc;
+  const double2* ph = a.ph_dn + a.octant[b] * Kp;
+  const double2* bp = a.Bp + (static_cast<size_t>(a.parent[b]) * 6 + c) * Kp;
+  double2* out = a.Bm + (static_cast<size_t>(b) * 6 + c) * Kc;
+  for (int tc0 = 0; tc0 < a.ntc; tc0 += band_rows) {
+    const int rows = min(band_rows, a.ntc - tc0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < rows * a.npp; e += blockDim.x) {
+      const int r = e / a.npp, pp = e - r * a.npp;
+      const int tc = tc0 + r;
+      double2 v = c2(0.0, 0.0);
+      for (int q = a.th_ptr[tc]; q < a.th_ptr[tc + 1]; ++q) {
+        const int kp = a.th_src[q] * a.npp + pp;
+        v = cfmas(a.th_w[q], cmul(__ldg(ph + kp), __ldg(bp + kp)), v);
+      }
+      band[r * a.npp + pp] = v;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < rows * a.npc; e += blockDim.x) {
+      const int r = e / a.npc, pc = e - r * a.npc;
+      double2 v = c2(0.0, 0.0);
+      for (int q = a.ph_ptr[pc]; q < a.ph_ptr[pc + 1]; ++q) v = cfmas(a.ph_w[q], band[r * a.npp + a.ph_src[q]], v);
+      double2* o = out + (tc0 + r) * a.npc + pc;
+      *o = cadd(*o, v);
+    }
+  }
 }
 
 struct LeafArg {
@@ -258,42 +405,47 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
     const MediumLevel& leaf = P.ml[m][L];
     dim3 g(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads);
     agg_kernel<<<g, kThreads, 0, s>>>(P.d_Vs[m], P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, leaf.S);
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[1 + 3 * m], s));
+    if (ev) MLFMA_CUDA(cudaEventRecord(ev[1 + 4 * m], s));
     for (int l = L - 1; l >= 2; --l) {
       const MediumLevel& pm = P.ml[m][l];
       const MediumLevel& cm = P.ml[m][l + 1];
       UpArg a{cm.S, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
               pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
-      dim3 gu(P.lv[l].B, (pm.K + kThreads - 1) / kThreads);
+      dim3 gu(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6);
       up_kernel<<<gu, kThreads, 0, s>>>(a);
     }
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[2 + 3 * m], s));
+    if (ev) MLFMA_CUDA(cudaEventRecord(ev[2 + 4 * m], s));
+    // translations of every level (independent of each other) ...
     for (int l = 2; l <= L; ++l) {
       const MediumLevel& cm = P.ml[m][l];
-      DownArg a{};
-      a.S = cm.S;
-      a.Bm = cm.Bm;
-      a.far_ptr = P.lv[l].far_ptr;
-      a.far_idx = P.lv[l].far_idx;
-      a.far_off = P.lv[l].far_off;
-      a.off2vec = cm.off2vec;
-      a.tfw = cm.tfw;
-      a.K = cm.K;
-      if (l > 2) {
-        const MediumLevel& pm = P.ml[m][l - 1];
-        a.Bp = pm.Bm;
-        a.parent = P.lv[l].parent;
-        a.octant = P.lv[l].octant;
-        a.ph_dn = pm.ph_dn;
-        a.tr_ptr = cm.tr_ptr;
-        a.tr_kp = cm.tr_kp;
-        a.tr_w = cm.tr_w;
-        a.Kp = pm.K;
+      if (P.tuning.m2l_variant == 1) {
+        M2lTileArg a{cm.S, cm.Bm, P.lv[l - 1].child_begin, P.lv[l].usrc_ptr, P.lv[l].usrc, P.lv[l].coord,
+                     cm.off2vec, cm.tfw, cm.K};
+        dim3 gd(P.lv[l - 1].B, (cm.K + kTileDirs - 1) / kTileDirs);
+        m2l_tile_kernel<<<gd, kTileDirs * kTileWarps, 0, s>>>(a);
+      } else {
+        M2lArg a{cm.S, cm.Bm, P.lv[l].far_ptr, P.lv[l].far_idx, P.lv[l].far_off, cm.off2vec, cm.tfw, cm.K};
+        dim3 gd(P.lv[l].B, (cm.K + kThreads - 1) / kThreads);
+        m2l_kernel<<<gd, kThreads, 0, s>>>(a);
       }
-      dim3 gd(P.lv[l].B, (cm.K + kThreads - 1) / kThreads);
-      down_kernel<<<gd, kThreads, 0, s>>>(a);
     }
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[3 + 3 * m], s));
+    if (ev) MLFMA_CUDA(cudaEventRecord(ev[3 + 4 * m], s));
+    // ... then the downward chain: level l receives level l-1 once that is final
+    for (int l = 3; l <= L; ++l) {
+      const MediumLevel& cm = P.ml[m][l];
+      const MediumLevel& pm = P.ml[m][l - 1];
+      if (P.tuning.l2l_variant == 1 && pm.nph <= kL2lMaxPhi) {
+        L2lSepArg b{cm.Bm,      pm.Bm,     P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.thT_ptr,
+                    cm.thT_src, cm.thT_w,  cm.phT_ptr,     cm.phT_src,     cm.phT_w, cm.nth,
+                    cm.nph,     pm.nth,    pm.nph};
+        l2l_sep_kernel<<<dim3(P.lv[l].B, 6), 256, 0, s>>>(b);
+      } else {
+        L2lArg b{cm.Bm, pm.Bm, P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.tr_ptr, cm.tr_kp, cm.tr_w, cm.K, pm.K};
+        dim3 gl(P.lv[l].B, (cm.K + kThreads - 1) / kThreads, 6);
+        l2l_kernel<<<gl, kThreads, 0, s>>>(b);
+      }
+    }
+    if (ev) MLFMA_CUDA(cudaEventRecord(ev[4 + 4 * m], s));
   }
   LeafArg a{};
   for (int m = 0; m < 2; ++m) {
@@ -320,27 +472,26 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   const int warps = kThreads / 32;
   leaf_out_kernel<<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
   MLFMA_CUDA(cudaGetLastError());
-  if (ev) MLFMA_CUDA(cudaEventRecord(ev[7], s));
+  if (ev) MLFMA_CUDA(cudaEventRecord(ev[9], s));
 }
 
 }  // namespace mlfma
 
 namespace mlfma {
 // Sums the recorded stage times (ms) since the last read: out[0] aggregation,
-// out[1] interpolation up, out[2] translation + anterpolation down,
-// out[3] leaf testing + near field. Returns the number of applies covered.
-int read_stage_times(Plan& P, double out[4]) {
-  for (int i = 0; i < 4; ++i) out[i] = 0.0;
+// out[1] interpolation up, out[2] translation, out[3] anterpolation down,
+// out[4] leaf testing + near field. Returns the number of applies covered.
+int read_stage_times(Plan& P, double out[kStages]) {
+  for (int i = 0; i < kStages; ++i) out[i] = 0.0;
   const int n = static_cast<int>(P.prof.used);
   for (int a = 0; a < n; ++a) {
     auto& e = P.prof.sets[a];
-    MLFMA_CUDA(cudaEventSynchronize(e[7]));
-    float t[7];
-    for (int i = 0; i < 7; ++i) MLFMA_CUDA(cudaEventElapsedTime(&t[i], e[i], e[i + 1]));
-    out[0] += t[0] + t[3];
-    out[1] += t[1] + t[4];
-    out[2] += t[2] + t[5];
-    out[3] += t[6];
+    MLFMA_CUDA(cudaEventSynchronize(e[StageProfiler::kEvents - 1]));
+    float t[StageProfiler::kEvents - 1];
+    for (int i = 0; i + 1 < StageProfiler::kEvents; ++i) MLFMA_CUDA(cudaEventElapsedTime(&t[i], e[i], e[i + 1]));
+    for (int m = 0; m < 2; ++m)
+      for (int k = 0; k < 4; ++k) out[k] += t[4 * m + k];
+    out[4] += t[8];
   }
   P.prof.used = 0;
   return n;

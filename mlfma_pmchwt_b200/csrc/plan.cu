@@ -59,6 +59,7 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   auto P = std::make_unique<Plan>();
   P->device = prm.device;
   P->verbose = prm.verbose;
+  P->tf_complex_argument = prm.tf_complex_argument;
   P->mesh = std::move(mesh);
   if (!(prm.freq > 0) || !(prm.leaf_coeff > 0)) throw std::invalid_argument("freq and leaf_coeff must be positive");
   if (!quad_rule(prm.gauss, P->quad)) throw std::invalid_argument("unsupported triangle rule");
@@ -154,6 +155,29 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
       D.far_ptr = P->upload(Lv.far_ptr);
       D.far_idx = P->upload(Lv.far_idx);
       D.far_off = P->upload(Lv.far_off);
+      std::vector<int> coord(3 * static_cast<size_t>(Lv.size()));
+      for (int b = 0; b < Lv.size(); ++b) {
+        coord[3 * b] = Lv.ix[b];
+        coord[3 * b + 1] = Lv.iy[b];
+        coord[3 * b + 2] = Lv.iz[b];
+      }
+      D.coord = P->upload(coord);
+      // per parent: children of the parent's 27-neighbourhood (itself included)
+      const Level& Pl = T.lv[l - 1];
+      std::vector<int> uptr(Pl.size() + 1, 0), usrc;
+      std::vector<int> tmp;
+      for (int p = 0; p < Pl.size(); ++p) {
+        tmp.clear();
+        for (int e = Pl.near_ptr[p]; e <= Pl.near_ptr[p + 1]; ++e) {
+          const int q = e < Pl.near_ptr[p + 1] ? Pl.near_idx[e] : p;
+          for (int c = Pl.child_begin[q]; c < Pl.child_begin[q + 1]; ++c) tmp.push_back(c);
+        }
+        std::sort(tmp.begin(), tmp.end());
+        usrc.insert(usrc.end(), tmp.begin(), tmp.end());
+        uptr[p + 1] = static_cast<int>(usrc.size());
+      }
+      D.usrc_ptr = P->upload(uptr);
+      D.usrc = P->upload(usrc);
     }
   }
   for (int m = 0; m < 2; ++m) {
@@ -199,6 +223,30 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
         M.tr_ptr = P->upload(cnt);
         M.tr_kp = P->upload(kps);
         M.tr_w = P->upload(ws);
+        // separable transposes of the two 1-D stencils
+        auto transpose1d = [&](const std::vector<int>& idx, const std::vector<double>& w, int nsrc, int ndst,
+                               int*& d_ptr, int*& d_src, double*& d_w) {
+          std::vector<int> ptr(ndst + 1, 0), src;
+          std::vector<double> wt;
+          for (int q = 0; q < nsrc; ++q)
+            for (int i = 0; i < 3; ++i) ptr[idx[3 * q + i] + 1]++;
+          for (int d = 0; d < ndst; ++d) ptr[d + 1] += ptr[d];
+          src.resize(ptr[ndst]);
+          wt.resize(ptr[ndst]);
+          std::vector<int> f(ptr.begin(), ptr.end() - 1);
+          for (int q = 0; q < nsrc; ++q)
+            for (int i = 0; i < 3; ++i) {
+              const int d = idx[3 * q + i];
+              src[f[d]] = q;
+              wt[f[d]] = w[3 * q + i];
+              f[d]++;
+            }
+          d_ptr = P->upload(ptr);
+          d_src = P->upload(src);
+          d_w = P->upload(wt);
+        };
+        transpose1d(I.tidx, I.lt, Pm.nth, M.nth, M.thT_ptr, M.thT_src, M.thT_w);
+        transpose1d(I.pidx, I.lp, Pm.nph, M.nph, M.phT_ptr, M.phT_src, M.phT_w);
       }
       // transfer factors over the offsets this level uses (Code/AlgoMLFMM.h:192-295)
       {
@@ -276,7 +324,10 @@ void Plan::tf_inputs(int m, int l, std::vector<double>& rhat, std::vector<int>& 
     for (double& v : r) v /= Rpq;
     const cplx kR = kw * Rpq;
     const int Lt = std::min(M.L, static_cast<int>(std::ceil(std::abs(kR))));
-    hankel2_array(Lt, std::abs(kR), h2);
+    if (tf_complex_argument)
+      hankel2_array_complex(Lt, kR, h2);  // not the reference: see PlanParams::tf_complex_argument
+    else
+      hankel2_array(Lt, std::abs(kR), h2);
     rhat.insert(rhat.end(), r, r + 3);
     hoff.push_back(static_cast<int>(h2all.size()));
     hL.push_back(Lt);

@@ -40,6 +40,14 @@ struct MediumLevel {
   int* tr_ptr = nullptr;       // [K+1]
   int* tr_kp = nullptr;
   double* tr_w = nullptr;
+  // the same, separable: child theta row -> (parent theta row, weight),
+  // child phi column -> (parent phi column, weight)
+  int* thT_ptr = nullptr;
+  int* thT_src = nullptr;
+  double* thT_w = nullptr;
+  int* phT_ptr = nullptr;
+  int* phT_src = nullptr;
+  double* phT_w = nullptr;
   // host copies
   Grid grid;
   Interp interp;               // this level from level+1 (levels 2..maxL-1)
@@ -55,12 +63,22 @@ struct DevLevel {
   int* far_idx = nullptr;
   int* far_off = nullptr;
   long long far_pairs = 0;
+  int* coord = nullptr;        // [3 * B] integer box coordinates
+  int* usrc_ptr = nullptr;     // per parent box (level - 1): union of its children's
+  int* usrc = nullptr;         //   interaction sources at this level (ascending)
+};
+
+// Kernel choices a plan can be tuned with (mlfma_set_tuning).
+struct Tuning {
+  int m2l_variant = 1;         // 0: one thread per (box, direction); 1: sibling-group tiles
+  int l2l_variant = 1;         // 0: 2-D transposed taps per child direction; 1: separable
 };
 
 // Per-apply CUDA events between stage groups, recorded on the launching
-// stream: [m1 agg | m1 up | m1 down | m2 agg | m2 up | m2 down | leaf_out].
+// stream: [m1 agg | m1 up | m1 m2l | m1 l2l | m2 agg | m2 up | m2 m2l | m2 l2l | leaf_out].
+constexpr int kStages = 5;
 struct StageProfiler {
-  static constexpr int kEvents = 8;
+  static constexpr int kEvents = 10;
   bool on = false;
   std::vector<std::array<cudaEvent_t, kEvents>> sets;
   size_t used = 0;
@@ -76,11 +94,13 @@ struct Plan {
   int maxL = 0;
   int device = 0;
   int verbose = 0;
+  int tf_complex_argument = 0;
   cplx k1, k2, eta1, eta2, etai, epsr, mur;
   double lambda = 0.0, freq = 0.0;
   double setup_seconds = 0.0;
   std::vector<MediumLevel> ml[2];   // index = physical level (0..maxL), used 2..maxL
   std::vector<DevLevel> lv;         // index = physical level
+  Tuning tuning;
   // ---- device geometry
   double* d_xyz = nullptr;          // [3 * points]
   int* d_face_v = nullptr;          // [3 * faces]
@@ -155,6 +175,10 @@ struct PlanParams {
   int gauss = 7;
   int device = 0;
   int verbose = 0;
+  // 0: transfer factors with h2_l(|kR|), the reference's choice even for a
+  // lossy (complex) k (Code/AlgoMLFMM.h:262-265). 1: h2_l(kR) with the
+  // complex argument, consistent with the complex-k shifts and near field.
+  int tf_complex_argument = 0;
 };
 std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& p);
 
@@ -165,6 +189,6 @@ void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& 
                      const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s);
 void launch_near(Plan& P, cudaStream_t s);
 void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s);
-int read_stage_times(Plan& P, double out[4]);
+int read_stage_times(Plan& P, double out[kStages]);
 
 }  // namespace mlfma

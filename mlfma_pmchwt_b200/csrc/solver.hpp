@@ -10,6 +10,7 @@ struct SolveStats {
   int iterations = 0;
   int restarts = 0;
   int matvecs = 0;
+  int near_products = 0;
   double rel_residual = 0.0;
   double seconds = 0.0;
 };
@@ -18,6 +19,14 @@ struct SolveStats {
 // host complex128 [2N]. Returns true when converged.
 bool gmres_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, double tol_abs, double tol_rel,
                  SolveStats& st, std::vector<double>& history);
+
+// Flexible GMRES(mr) whose right preconditioner is inner_its GMRES steps on
+// the near-field matrix alone (fgmres.cu); inner_its = 0 gives plain GMRES.
+bool fgmres_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, double tol_abs, double tol_rel,
+                  int inner_its, SolveStats& st, std::vector<double>& history);
+
+// w = Z_near x on device vectors (complex128 [2N]).
+void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s);
 
 void rhs_pmchwt(Plan& P, const double kinc[3], const double einc[3], const double hinc[3], double* V);
 

@@ -48,6 +48,9 @@ CASES = {
     "sphere_s3_lossy": (lambda: M.icosphere(3, 1.0), complex(2.5, -0.1), 0.3),
     # triaxial ellipsoid
     "ellipsoid_s3": (lambda: M.ellipsoid(3, 0.8 * LAMBDA, 0.5 * LAMBDA, 0.35 * LAMBDA), 3.0 - 0.05j, 0.25),
+    # deep trees (maxLevel 5) at small cost: small leaf boxes
+    "sphere_s4_deep": (lambda: M.icosphere(4, 1.5), 2.5 - 0.1j, 0.12),
+    "ellipsoid_s4_deep": (lambda: M.ellipsoid(4, 2.0, 1.4, 1.0), 4.0, 0.15),
 }
 
 

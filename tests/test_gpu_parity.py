@@ -28,7 +28,7 @@ def gpu_op(case_files, name):
     return _ops[name]
 
 
-CASES = ["sphere_s2", "sphere_s3", "sphere_s3_lossy", "ellipsoid_s3"]
+CASES = ["sphere_s2", "sphere_s3", "sphere_s3_lossy", "ellipsoid_s3", "sphere_s4_deep", "ellipsoid_s4_deep"]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -96,7 +96,7 @@ def test_matvec_matches_reference(case_files, ref_ops, name):
     assert rel(op.apply_ax(ones), ref.apply(ones)) < MATVEC_TOL
 
 
-@pytest.mark.parametrize("name", ["sphere_s3"])
+@pytest.mark.parametrize("name", ["sphere_s3", "sphere_s4_deep"])
 def test_stage_arrays(case_files, ref_ops, name):
     """Aggregated (Sm) and incoming (Bm) patterns per level and box."""
     from mlfma_pmchwt_b200 import mesh as M
@@ -202,3 +202,22 @@ def test_error_paths_on_device_plan(case_files):
     with pytest.raises(MlfmaError) as e:
         op.apply_device(0, 0)
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("name", ["sphere_s3", "ellipsoid_s3"])
+def test_translation_variants_agree(case_files, ref_ops, name):
+    """Both translation kernels (per-box and sibling-group tiles) give the
+    reference's matvec, and agree with each other to rounding."""
+    from mlfma_pmchwt_b200 import mesh as M
+    op, ref = gpu_op(case_files, name), ref_ops(name)
+    x = M.unit_disk_vector(op.n, 6)
+    wr = ref.apply(x)
+    out = {}
+    for v in (0, 1):
+        op.set_tuning("m2l.variant", v)
+        out[v] = op.apply_ax(x)
+        assert rel(out[v], wr) < MATVEC_TOL
+    assert rel(out[1], out[0]) < 1e-13
+    res = op.autotune(2)
+    assert res["m2l.variant"] in (0, 1) and all(t > 0 for t in res["variant_ms"])
+    assert rel(op.apply_ax(x), wr) < MATVEC_TOL
