@@ -37,6 +37,18 @@ UNIT = "matvec/s"
 FREQ = 3.0e8
 
 
+def launches_per_apply(max_level: int, tune: dict) -> int:
+    """Kernels one operator apply launches: the aggregation (one launch for
+    both media with agg variant 1, else one per medium); per medium one
+    interpolation per level pair, the translations (one launch for every
+    level with m2l variants 2 and 3, else one per level) and one anterpolation per
+    level pair; then the leaf testing + near-field kernel."""
+    lv = max_level - 2
+    m2l = 1 if tune["m2l.variant"] in (2, 3) else lv + 1
+    agg = 1 if tune.get("agg.variant", 0) == 1 else 2
+    return agg + 2 * (lv + m2l + lv) + 1
+
+
 def workload(args):
     from mlfma_pmchwt_b200 import mesh as M
     lam = M.wavelength(FREQ)
@@ -208,6 +220,28 @@ def run_reference_arm(args):
     return 0
 
 
+def parse_tuning(spec: str) -> dict | None:
+    """'auto' -> None (autotune); else 'key=value,...' fixed kernel variants."""
+    if spec == "auto":
+        return None
+    out = {}
+    for item in spec.split(","):
+        k, v = item.split("=")
+        out[k.strip()] = int(v)
+    return out
+
+
+def solve_record(st: dict, inner_its: int) -> dict:
+    rec = {"s_per_rhs": round(st["seconds"], 4), "iterations": st["iterations"], "converged": st["converged"],
+           "rel_residual": st["rel_residual"], "restart": 50, "tol": 1e-3, "matvecs": st["matvecs"]}
+    if inner_its:
+        rec["solver"] = f"FGMRES(50), right preconditioner = {inner_its} GMRES steps on the near field"
+        rec["near_products"] = st["near_products"]
+    else:
+        rec["solver"] = "GMRES(50)"
+    return rec
+
+
 def run_product(args):
     import torch
     from mlfma_pmchwt_b200 import MLFMM
@@ -234,7 +268,13 @@ def run_product(args):
     def step():
         op.apply_device(x.data_ptr(), w.data_ptr(), sp)
 
-    tune = op.autotune(3)
+    fixed = parse_tuning(args.tuning)
+    if fixed is None:
+        tune = op.autotune(3)
+    else:
+        for k, v in fixed.items():
+            op.set_tuning(k, v)
+        tune = {k: op.get_tuning(k) for k, _ in op.TUNING_KEYS}
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize(dev)
@@ -293,127 +333,33 @@ def run_product(args):
                 "matvec_bytes": sum(sb.values()),
                 "matvec_frac": round(sum(sb.values()) / (ms_per_step / 1000.0) / 1e9 / peak, 4)}
 
-    # solve of the plane-wave excitation (x-polarised, incident along -z) to
-    # 1e-3: flexible GMRES(50) with the near-field preconditioner, and the
-    # plain GMRES(50) of the reference for comparison (capped iterations)
+    # Solves of the plane-wave excitation (x-polarised, incident along -z) to
+    # 1e-3 relative residual. (1) The reference's operator (real-argument
+    # transfer factors, as Code/AlgoMLFMM.h:259-281 evaluates them for the
+    # lossy medium too) with FGMRES(50) + near-field preconditioner;
+    # (2) the same with complex-argument transfer factors h2_l(k2 R), which
+    # the lossy medium needs for the far field to match its near field.
     solve = None
     if args.solve_its > 0:
         from mlfma_pmchwt_b200 import plane_wave
         V = op.compute_v_pmchwt(*plane_wave(0.0, 0.0, 0.0))
-        xs, st = op.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
-                                  inner_its=args.inner_its)
-        solve = {"s_per_rhs": round(st["seconds"], 4), "iterations": st["iterations"],
-                 "converged": st["converged"], "rel_residual": st["rel_residual"], "restart": 50, "tol": 1e-3,
-                 "solver": f"FGMRES(50), right preconditioner = {args.inner_its} GMRES steps on the near field",
-                 "matvecs": st["matvecs"], "near_products": st["near_products"], "itr_max": args.solve_its}
+        _, st = op.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
+                                 inner_its=args.inner_its)
+        solve = {"reference_transfer": solve_record(st, args.inner_its)}
         if args.plain_its > 0:
-            xp, sp_ = op.matrix_solver(V, itr_max=args.plain_its, mr=50, tol_abs=1e-8, tol_rel=1e-3)
-            solve["plain_gmres"] = {"s": round(sp_["seconds"], 4), "iterations": sp_["iterations"],
-                                    "converged": sp_["converged"], "rel_residual": sp_["rel_residual"]}
-
-    line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / base["value"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": wl["name"], "parallelism": "openmp", "l2": "inputs larger than L2"},
-            "impl": "reference", "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
-    return 0
-
-
-def run_product(args):
-    import torch
-    from mlfma_pmchwt_b200 import MLFMM
-    from mlfma_pmchwt_b200 import mesh as M
-
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    wl = workload(args)
-    m = M.icosphere(wl["sub"], wl["radius"])
-    t0 = time.perf_counter()
-    op = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local)
-    setup_s = time.perf_counter() - t0
-    n = op.n
-    x_host = M.unit_disk_vector(n, 0)
-    x = torch.from_numpy(x_host).to(dev)
-    w = torch.empty(n, dtype=torch.complex128, device=dev)
-    # a dedicated stream: the legacy default stream has handle 0, which the C
-    # ABI reads as "the plan's own stream"
-    stream = torch.cuda.Stream(dev)
-    torch.cuda.set_stream(stream)
-    sp = stream.cuda_stream
-
-    def step():
-        op.apply_device(x.data_ptr(), w.data_ptr(), sp)
-
-    tune = op.autotune(3)
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize(dev)
-
-    # timed region: device time, max over ranks
-    op.profile(True)
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.4)
-    barrier(world)
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier(world)
-    clk = clocks.stop()
-    ms_local = e0.elapsed_time(e1)
-    stage_ms, napp = op.stage_times()
-    op.profile(False)
-    ms_total = allreduce_max(ms_local, world, dev)
-    ms_per_step = ms_total / args.steps
-    value = world * args.steps / (ms_total / 1000.0)
-
-    # end to end through the C ABI with pinned host buffers
-    xh = torch.from_numpy(x_host).pin_memory()
-    wh = torch.empty(n, dtype=torch.complex128).pin_memory()
-    xh_np, wh_np = xh.numpy(), wh.numpy()
-    for _ in range(2):
-        op._lib.mlfma_apply(op._h, n, xh_np.ctypes.data_as(_dp_t()), wh_np.ctypes.data_as(_dp_t()))
-    barrier(world)
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        rc = op._lib.mlfma_apply(op._h, n, xh_np.ctypes.data_as(_dp_t()), wh_np.ctypes.data_as(_dp_t()))
-        if rc != 0:
-            raise RuntimeError(op._lib.mlfma_last_error().decode())
-    e2e_s = allreduce_max(time.perf_counter() - t, world, dev)
-    barrier(world)
-    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * 16,
-           "d2h_bytes_per_step": n * 16}
-
-    # roofline of the dominant stage (HBM-bound FP64 path)
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    sb = stage_bytes(op)
-    per_apply_ms = {k: v / max(napp, 1) for k, v in stage_ms.items()}
-    dom = max(per_apply_ms, key=per_apply_ms.get)
-    achieved = sb[dom] / (per_apply_ms[dom] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": None,
-                "algorithmic_bytes": sb[dom],
-                "stage_ms_per_apply": {k: round(v, 4) for k, v in per_apply_ms.items()},
-                "matvec_bytes": sum(sb.values()),
-                "matvec_frac": round(sum(sb.values()) / (ms_per_step / 1000.0) / 1e9 / peak, 4)}
-
-    # one GMRES(50) solve of the plane-wave excitation, capped iterations
-    solve = None
-    if args.solve_its > 0:
-        from mlfma_pmchwt_b200 import plane_wave
-        V = op.compute_v_pmchwt(*plane_wave(0.0, 0.0, 0.0))
-        xs, st = op.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3)
-        solve = {"s_per_rhs": round(st["seconds"], 4), "iterations": st["iterations"], "converged": st["converged"],
-                 "rel_residual": st["rel_residual"], "restart": 50, "tol": 1e-3, "itr_max": args.solve_its}
+            _, sp_ = op.matrix_solver(V, itr_max=args.plain_its, mr=50, tol_abs=1e-8, tol_rel=1e-3)
+            solve["reference_transfer_plain_gmres"] = solve_record(sp_, 0)
+        if wl["eps"].imag != 0.0:
+            op.close()
+            opc = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local,
+                        tf_complex_argument=True)
+            for k, v in tune.items():
+                if not k.endswith("_ms"):
+                    opc.set_tuning(k, v)
+            _, sc = opc.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
+                                      inner_its=args.inner_its)
+            solve["complex_transfer"] = solve_record(sc, args.inner_its)
+            op = opc
 
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -421,10 +367,9 @@ def run_product(args):
             "config": {"workload": wl["name"], "unknowns": n, "max_level": op.max_level,
                        "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
                        "setup_s": round(setup_s, 2), "device_bytes": op.info.bytes_device,
-                       "tuning": {"m2l.variant": tune["m2l.variant"],
-                                  "variant_ms": [round(v, 4) for v in tune["variant_ms"]]}},
+                       "tuning": tune},
             "e2e": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in e2e.items()},
-            "gpu_launches": args.steps * (2 * (1 + 3 * (op.max_level - 2) + 1) + 1),
+            "gpu_launches": args.steps * launches_per_apply(op.max_level, tune),
             "roofline": roofline, "clocks": clk}
     if solve:
         line["solve"] = solve
@@ -458,6 +403,8 @@ def main(argv=None):
     ap.add_argument("--plain-its", type=int, default=300, help="iteration cap of the plain GMRES comparison")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference matvecs to time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="auto",
+                    help="'auto' (autotune) or fixed kernel variants, e.g. m2l.variant=2,up.variant=1")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference_arm(args)

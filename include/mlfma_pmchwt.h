@@ -126,6 +126,19 @@ MLFMA_API int mlfma_apply(mlfma_plan* plan, int n, const double* x, double* w);
  * (cudaStream_t passed as void*; NULL = the plan's stream). Asynchronous. */
 MLFMA_API int mlfma_apply_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream);
 
+/* Batched apply: w[j] = A x[j] for R right-hand sides stored one after the
+ * other (x[j] at x + 2 n j doubles, complex128 interleaved, n = 2N each).
+ * The reference applies its AxFunc (Code/GMRES.h:53-66, the ax closure of
+ * Code/MLFMM.cpp:189-368) once per right-hand side; here the leaf radiation /
+ * receive patterns and the near-field entries are read once per group of up
+ * to 16 right-hand sides. Each w[j] equals the single apply's result.
+ * The first call on a plan allocates the leaf-level workspace of min(R, 16)
+ * right-hand sides (about 2 x leaf boxes x 6 x (K1+K2) x 16 bytes each) plus,
+ * for the host-pointer form, 2 x 16 staging vectors. Not re-entrant per plan. */
+MLFMA_API int mlfma_apply_batch(mlfma_plan* plan, int n, int R, const double* x, double* w);
+MLFMA_API int mlfma_apply_batch_device(mlfma_plan* plan, int n, int R, const void* x_dev, void* w_dev,
+                                       void* stream);
+
 /* Stage timing (no counterpart in the reference, whose timers are
  * std::chrono prints): with on != 0 every apply records CUDA events on its
  * stream between stage groups; mlfma_profile_read sums them since the last
@@ -134,12 +147,28 @@ MLFMA_API int mlfma_apply_device(mlfma_plan* plan, int n, const void* x_dev, voi
 MLFMA_API int mlfma_profile(mlfma_plan* plan, int on);
 MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applies);
 
-/* Kernel variants of a plan (no counterpart in the reference). key
- * "m2l.variant": 0 = one thread per (box, direction) over the interaction
- * list, 1 = sibling-group tiles staging the shared sources in shared memory
- * (default). mlfma_autotune times each variant over `applies` applies of the
- * plan's own operator (device vectors owned by the plan) and keeps the
- * fastest; variant_ms receives the per-apply time of each (may be NULL). */
+/* Kernel variants of a plan (no counterpart in the reference). Keys and values:
+ *   "m2l.variant"  0 = one thread per (box, direction) over the interaction
+ *                  list; 1 = sibling-group tiles staging the shared sources in
+ *                  shared memory; 2 = octant registers: one thread per
+ *                  (parent, direction, J|M) holds all 8 children and applies
+ *                  each source of the siblings' union once, every level of a
+ *                  medium in one launch; 3 = warp per box, 8 Morton-consecutive
+ *                  boxes per CTA sharing their source patterns through L1, every
+ *                  level of a medium in one launch.
+ *   "up.variant"   0 = 9-tap gather per parent direction; 1 = separable
+ *                  phi-then-theta interpolation in bands of theta rows (default).
+ *   "l2l.variant"  0 = transposed 9-tap gather per child direction;
+ *                  1 = separable transposed theta-then-phi (default).
+ *   "agg.variant"  0 = one thread per (leaf box, direction), one launch per
+ *                  medium; 1 = one CTA per (leaf box, medium) streaming the
+ *                  box's contiguous pattern block, both media in one launch
+ *                  (default).
+ * mlfma_autotune times the values of each key in that order (the others held
+ * at their current values) over `applies` applies of the plan's own operator
+ * (device vectors owned by the plan) and keeps the fastest; variant_ms (may be
+ * NULL) receives the per-apply ms of every value, keys in that order
+ * (10 entries: m2l 0-3, up 0-1, l2l 0-1, agg 0-1). */
 MLFMA_API int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value);
 MLFMA_API int mlfma_get_tuning(const mlfma_plan* plan, const char* key);
 MLFMA_API int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms);
@@ -166,6 +195,20 @@ MLFMA_API int mlfma_gmres(mlfma_plan* plan, int n, double* x, const double* rhs,
 MLFMA_API int mlfma_fgmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr,
                            double tol_abs, double tol_rel, int inner_its, mlfma_solve_stats* stats,
                            double* history, int history_cap);
+
+/* Lockstep FGMRES of R right-hand sides (x, rhs: R vectors of n = 2N
+ * complex128 one after the other; x holds the initial guesses and receives
+ * the solutions). Per system the iteration, stopping rule and divergence
+ * abort are mlfma_fgmres's (itself MGMRES::mgmres, Code/GMRES.h:65-217, with
+ * the optional near-field right preconditioner); the reference solves its
+ * incidences one after the other (Code/RCS.h:467-468). Here every Arnoldi
+ * step applies the operator to all systems still iterating at once
+ * (mlfma_apply_batch), and the inner near-field products and the
+ * Gram-Schmidt steps are batched the same way. stats: R entries (seconds =
+ * the whole batch, history_len = 0). Returns MLFMA_OK when every system
+ * converged, MLFMA_ERR_NOT_CONVERGED otherwise. */
+MLFMA_API int mlfma_fgmres_batch(mlfma_plan* plan, int n, int R, double* x, const double* rhs, int itr_max, int mr,
+                                 double tol_abs, double tol_rel, int inner_its, mlfma_solve_stats* stats);
 
 /* w = Z_near x on device vectors: the near-field rows alone (the product of
  * Code/MLFMM.cpp:353-366 without the far field). Asynchronous on stream. */

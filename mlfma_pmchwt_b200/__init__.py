@@ -78,6 +78,8 @@ SIGNATURES = {
     "mlfma_plan_info": (C.c_int, [_P, C.POINTER(Info)]),
     "mlfma_apply": (C.c_int, [_P, C.c_int, _DP, _DP]),
     "mlfma_apply_device": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "mlfma_apply_batch": (C.c_int, [_P, C.c_int, C.c_int, _DP, _DP]),
+    "mlfma_apply_batch_device": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P]),
     "mlfma_profile": (C.c_int, [_P, C.c_int]),
     "mlfma_profile_read": (C.c_int, [_P, _DP, C.POINTER(C.c_int)]),
     "mlfma_set_tuning": (C.c_int, [_P, C.c_char_p, C.c_int]),
@@ -87,6 +89,8 @@ SIGNATURES = {
                               C.POINTER(SolveStats), _DP, C.c_int]),
     "mlfma_fgmres": (C.c_int, [_P, C.c_int, _DP, _DP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                C.POINTER(SolveStats), _DP, C.c_int]),
+    "mlfma_fgmres_batch": (C.c_int, [_P, C.c_int, C.c_int, _DP, _DP, C.c_int, C.c_int, C.c_double, C.c_double,
+                                     C.c_int, C.POINTER(SolveStats)]),
     "mlfma_apply_near_device": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mlfma_rhs_pmchwt": (C.c_int, [_P, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt": (C.c_int, [_P, _DP, C.c_int, _DP, _DP, _DP, _DP]),
@@ -264,17 +268,42 @@ class MLFMM:
         self._check(self._lib.mlfma_apply_device(self._h, self.n, C.c_void_p(x_ptr), C.c_void_p(w_ptr),
                                                  C.c_void_p(stream or 0)))
 
+    def apply_batch(self, X) -> np.ndarray:
+        """W[j] = A X[j] for the rows of X (host, complex128 [R, 2N]); patterns
+        and near-field entries are read once per group of 16 right-hand sides."""
+        X = np.ascontiguousarray(X, dtype=np.complex128)
+        if X.ndim != 2 or X.shape[1] != self.n:
+            raise ValueError(f"X must have shape (R, {self.n})")
+        W = np.empty_like(X)
+        self._check(self._lib.mlfma_apply_batch(self._h, self.n, X.shape[0], _dp(X.view(np.float64)),
+                                                _dp(W.view(np.float64))))
+        return W
+
+    def apply_batch_device(self, R: int, x_ptr: int, w_ptr: int, stream: int | None = None):
+        """Batched apply on device pointers (complex128 [R, 2N]); asynchronous on `stream`."""
+        self._check(self._lib.mlfma_apply_batch_device(self._h, self.n, int(R), C.c_void_p(x_ptr),
+                                                       C.c_void_p(w_ptr), C.c_void_p(stream or 0)))
+
     def set_tuning(self, key: str, value: int):
         self._check(self._lib.mlfma_set_tuning(self._h, key.encode(), int(value)))
 
     def get_tuning(self, key: str) -> int:
         return self._check(self._lib.mlfma_get_tuning(self._h, key.encode()))
 
+    TUNING_KEYS = (("m2l.variant", 4), ("up.variant", 2), ("l2l.variant", 2), ("agg.variant", 2))
+
     def autotune(self, applies: int = 3) -> dict:
-        """Times each m2l variant on this plan and keeps the fastest."""
-        ms = np.zeros(2)
+        """Times the values of each tuning key on this plan (one key at a
+        time) and keeps the fastest; returns the choice and the per-apply ms
+        of every value tried."""
+        ms = np.zeros(sum(c for _, c in self.TUNING_KEYS))
         self._check(self._lib.mlfma_autotune(self._h, int(applies), _dp(ms)))
-        return {"m2l.variant": self.get_tuning("m2l.variant"), "variant_ms": ms.tolist()}
+        out, o = {}, 0
+        for key, cnt in self.TUNING_KEYS:
+            out[key] = self.get_tuning(key)
+            out[key + "_ms"] = [round(float(v), 4) for v in ms[o:o + cnt]]
+            o += cnt
+        return out
 
     STAGES = ("aggregation", "interpolation_up", "translation", "anterpolation_down", "leaf_testing_near")
 
@@ -312,6 +341,27 @@ class MLFMM:
                      converged=bool(st.converged), rel_residual=st.rel_residual, seconds=st.seconds,
                      near_products=st.near_products, history=hist[: st.history_len].copy())
         return x, stats
+
+    def matrix_solver_batch(self, rhs, x0=None, itr_max: int | None = None, mr: int = 50, tol_abs: float = 1e-8,
+                            tol_rel: float = 1e-4, inner_its: int = 0):
+        """Lockstep (F)GMRES of the R rows of rhs (complex128 [R, 2N]):
+        per system matrix_solver(..., inner_its) with every operator apply,
+        near-field product and Gram-Schmidt step batched over the systems
+        still iterating (mlfma_fgmres_batch). Returns (X [R, 2N], list of
+        per-system stats dicts)."""
+        B = np.ascontiguousarray(rhs, dtype=np.complex128)
+        if B.ndim != 2 or B.shape[1] != self.n:
+            raise ValueError(f"rhs must have shape (R, {self.n})")
+        R = B.shape[0]
+        X = np.zeros_like(B) if x0 is None else np.ascontiguousarray(x0, dtype=np.complex128).copy()
+        itr_max = self.n if itr_max is None else int(itr_max)
+        st = (SolveStats * R)()
+        rc = self._lib.mlfma_fgmres_batch(self._h, self.n, R, _dp(X.view(np.float64)), _dp(B.view(np.float64)),
+                                          itr_max, mr, tol_abs, tol_rel, int(inner_its), st)
+        self._check(rc)
+        stats = [dict(iterations=s.iterations, restarts=s.restarts, matvecs=s.matvecs, converged=bool(s.converged),
+                      rel_residual=s.rel_residual, seconds=s.seconds, near_products=s.near_products) for s in st]
+        return X, stats
 
     def apply_near_device(self, x_ptr: int, w_ptr: int, stream: int | None = None):
         """w = Z_near x on device pointers (the near-field rows alone)."""

@@ -32,6 +32,14 @@ NVCC_FLAGS = ARCH + [
 ]
 
 
+# Per-file flags. The near-field integrals take branches on near-zero
+# geometric quantities against absolute thresholds (the singular-term
+# extraction of Code/Operator.h); fused multiply-adds change those quantities
+# in the last bits and can flip a branch, so that file is compiled with
+# separately rounded multiplies and adds, like the reference's own build.
+FILE_FLAGS = {"setup_kernels.cu": ["-fmad=false"]}
+
+
 def nvcc() -> str:
     cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     if not Path(cand).exists():
@@ -58,7 +66,7 @@ def _compile(src: Path, force: bool) -> Path:
     newest_dep = max(p.stat().st_mtime for p in headers() + [src])
     if not force and obj.exists() and obj.stat().st_mtime >= newest_dep:
         return obj
-    cmd = [nvcc(), "-ccbin", host_cxx(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), "-ccbin", host_cxx(), *NVCC_FLAGS, *FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cpp":
         cmd[3:3] = ["-x", "cu"]
     subprocess.run(cmd, check=True)

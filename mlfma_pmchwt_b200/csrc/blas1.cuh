@@ -1,4 +1,5 @@
-// Length-n complex128 vector kernels for the Krylov solvers: Gram-Schmidt
+// Length-n complex128 vector kernels (internal linkage: one copy per including
+// file) for the Krylov solvers: Gram-Schmidt
 // projections against a block of basis vectors, updates, norms. Reductions
 // are two-stage (per-block partials, then one deterministic sum), so results
 // do not depend on scheduling.
@@ -41,7 +42,7 @@ __device__ __forceinline__ double2 block_sum(double2 v, double2* sh) {
 }
 
 // partial[blk * ldp + j] = sum over the block's rows of conj(V_j) w, j < nv
-__global__ void __launch_bounds__(kThreads) dots(const double2* __restrict__ V, long long n, int nv,
+static __global__ void __launch_bounds__(kThreads) dots(const double2* __restrict__ V, long long n, int nv,
                                                  const double2* __restrict__ w, double2* __restrict__ partial,
                                                  int ldp) {
   __shared__ double2 sh[kThreads / 32];
@@ -70,7 +71,7 @@ __global__ void __launch_bounds__(kThreads) dots(const double2* __restrict__ V, 
 }
 
 // out[j] = sum over blocks of partial[blk * ldp + j]
-__global__ void reduce(const double2* __restrict__ partial, int nblk, int ldp, int nv, double2* out) {
+static __global__ void reduce(const double2* __restrict__ partial, int nblk, int ldp, int nv, double2* out) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nv) return;
   double2 s = c2(0.0, 0.0);
@@ -79,7 +80,7 @@ __global__ void reduce(const double2* __restrict__ partial, int nblk, int ldp, i
 }
 
 // w -= sum_j V_j h[j]; optionally the block partials of ||w||^2 into partial[blk * ldp]
-__global__ void __launch_bounds__(kThreads) project_out(const double2* __restrict__ V, long long n, int nv,
+static __global__ void __launch_bounds__(kThreads) project_out(const double2* __restrict__ V, long long n, int nv,
                                                         const double2* __restrict__ h, double2* __restrict__ w,
                                                         int want_norm, double2* __restrict__ partial, int ldp) {
   __shared__ double2 hs[kMaxBasis];
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(kThreads) project_out(const double2* __restric
 }
 
 // block partials of ||v||^2 (or of ||b - w||^2 with r = b - w written when b != null)
-__global__ void __launch_bounds__(kThreads) norm2(const double2* __restrict__ b, const double2* __restrict__ w,
+static __global__ void __launch_bounds__(kThreads) norm2(const double2* __restrict__ b, const double2* __restrict__ w,
                                                   double2* __restrict__ r, long long n, double2* __restrict__ partial) {
   __shared__ double2 sh[kThreads / 32];
   double2 nrm = c2(0.0, 0.0);
@@ -116,13 +117,13 @@ __global__ void __launch_bounds__(kThreads) norm2(const double2* __restrict__ b,
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-__global__ void scale(const double2* __restrict__ src, double a, double2* __restrict__ dst, long long n) {
+static __global__ void scale(const double2* __restrict__ src, double a, double2* __restrict__ dst, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] = cscale(src[i], a);
 }
 
 // x (+)= sum_j V_j y[j]   (accumulate != 0: add to x, else overwrite)
-__global__ void combine(const double2* __restrict__ V, long long n, int m, const double2* __restrict__ y,
+static __global__ void combine(const double2* __restrict__ V, long long n, int m, const double2* __restrict__ y,
                         double2* __restrict__ x, int accumulate) {
   __shared__ double2 ys[kMaxBasis];
   for (int j = threadIdx.x; j < m; j += blockDim.x) ys[j] = y[j];

@@ -1,6 +1,7 @@
 // extern "C" boundary (include/mlfma_pmchwt.h). No exception crosses it:
 // every entry point maps failures onto status codes and records the message
 // for mlfma_last_error() on the calling thread.
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -176,6 +177,50 @@ int mlfma_apply_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, 
   });
 }
 
+int mlfma_apply_batch(mlfma_plan* plan, int n, int R, const double* x, double* w) {
+  if (!plan || !plan->p || !x || !w) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (R <= 0) return fail(MLFMA_ERR_ARG, "R must be positive");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    mlfma::reserve_batch(P, R);
+    if (P.xb_cap == 0) {
+      P.d_xb = P.alloc<double2>(static_cast<size_t>(mlfma::kBatchSlots) * n);
+      P.d_wb = P.alloc<double2>(static_cast<size_t>(mlfma::kBatchSlots) * n);
+      P.xb_cap = mlfma::kBatchSlots;
+    }
+    for (int g0 = 0; g0 < R; g0 += P.xb_cap) {
+      const int rn = std::min(P.xb_cap, R - g0);
+      const size_t bytes = static_cast<size_t>(rn) * n * sizeof(double2);
+      MLFMA_CUDA(cudaMemcpyAsync(P.d_xb, x + 2 * static_cast<size_t>(g0) * n, bytes, cudaMemcpyHostToDevice,
+                                 P.stream));
+      mlfma::apply_batch_device(P, rn, P.d_xb, n, P.d_wb, n, P.stream);
+      MLFMA_CUDA(cudaMemcpyAsync(w + 2 * static_cast<size_t>(g0) * n, P.d_wb, bytes, cudaMemcpyDeviceToHost,
+                                 P.stream));
+    }
+    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_apply_batch_device(mlfma_plan* plan, int n, int R, const void* x_dev, void* w_dev, void* stream) {
+  if (!plan || !plan->p || !x_dev || !w_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (R <= 0) return fail(MLFMA_ERR_ARG, "R must be positive");
+  if (x_dev == w_dev) return fail(MLFMA_ERR_ARG, "x and w must not alias");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    mlfma::reserve_batch(P, R);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::apply_batch_device(P, R, static_cast<const double2*>(x_dev), n, static_cast<double2*>(w_dev), n, s);
+    return MLFMA_OK;
+  });
+}
+
 int mlfma_profile(mlfma_plan* plan, int on) {
   if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
   if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
@@ -195,27 +240,40 @@ int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applies) {
   });
 }
 
+namespace {
+struct TuningKey {
+  const char* name;
+  int mlfma::Tuning::*field;
+  int count;  // values 0 .. count-1
+};
+constexpr TuningKey kTuningKeys[] = {
+    {"m2l.variant", &mlfma::Tuning::m2l_variant, 4},
+    {"up.variant", &mlfma::Tuning::up_variant, 2},
+    {"l2l.variant", &mlfma::Tuning::l2l_variant, 2},
+    {"agg.variant", &mlfma::Tuning::agg_variant, 2},
+};
+const TuningKey* find_key(const char* key) {
+  for (const TuningKey& k : kTuningKeys)
+    if (std::string(key) == k.name) return &k;
+  return nullptr;
+}
+}  // namespace
+
 int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value) {
   if (!plan || !plan->p || !key) return fail(MLFMA_ERR_ARG, "null argument");
-  const std::string k(key);
-  if (k == "m2l.variant") {
-    if (value < 0 || value > 1) return fail(MLFMA_ERR_ARG, "m2l.variant must be 0 or 1");
-    plan->p->tuning.m2l_variant = value;
-    return MLFMA_OK;
-  }
-  if (k == "l2l.variant") {
-    if (value < 0 || value > 1) return fail(MLFMA_ERR_ARG, "l2l.variant must be 0 or 1");
-    plan->p->tuning.l2l_variant = value;
-    return MLFMA_OK;
-  }
-  return fail(MLFMA_ERR_ARG, "unknown tuning key: " + k);
+  const TuningKey* k = find_key(key);
+  if (!k) return fail(MLFMA_ERR_ARG, std::string("unknown tuning key: ") + key);
+  if (value < 0 || value >= k->count)
+    return fail(MLFMA_ERR_ARG, std::string(key) + " must be in [0, " + std::to_string(k->count - 1) + "]");
+  plan->p->tuning.*(k->field) = value;
+  return MLFMA_OK;
 }
 
 int mlfma_get_tuning(const mlfma_plan* plan, const char* key) {
   if (!plan || !plan->p || !key) return fail(MLFMA_ERR_ARG, "null argument");
-  if (std::string(key) == "m2l.variant") return plan->p->tuning.m2l_variant;
-  if (std::string(key) == "l2l.variant") return plan->p->tuning.l2l_variant;
-  return fail(MLFMA_ERR_ARG, std::string("unknown tuning key: ") + key);
+  const TuningKey* k = find_key(key);
+  if (!k) return fail(MLFMA_ERR_ARG, std::string("unknown tuning key: ") + key);
+  return plan->p->tuning.*(k->field);
 }
 
 int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
@@ -230,10 +288,7 @@ int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
     MLFMA_CUDA(cudaMemsetAsync(P.d_x, 0, 2 * static_cast<size_t>(P.N) * sizeof(double2), P.stream));
     const bool prof = P.prof.on;
     P.prof.on = false;
-    double best = 1e300;
-    int best_v = P.tuning.m2l_variant;
-    for (int v = 0; v <= 1; ++v) {
-      P.tuning.m2l_variant = v;
+    auto time_apply = [&] {
       mlfma::apply_device(P, P.d_x, P.d_w, P.stream);  // warm-up
       MLFMA_CUDA(cudaEventRecord(e0, P.stream));
       for (int i = 0; i < applies; ++i) mlfma::apply_device(P, P.d_x, P.d_w, P.stream);
@@ -241,14 +296,25 @@ int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
       MLFMA_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
       MLFMA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      const double per = ms / applies;
-      if (variant_ms) variant_ms[v] = per;
-      if (per < best) {
-        best = per;
-        best_v = v;
+      return static_cast<double>(ms) / applies;
+    };
+    // one key at a time, the others held at their current (best so far) value
+    int slot = 0;
+    for (const TuningKey& k : kTuningKeys) {
+      double best = 1e300;
+      int best_v = P.tuning.*(k.field);
+      for (int v = 0; v < k.count; ++v) {
+        P.tuning.*(k.field) = v;
+        const double per = time_apply();
+        if (variant_ms) variant_ms[slot + v] = per;
+        if (per < best) {
+          best = per;
+          best_v = v;
+        }
       }
+      P.tuning.*(k.field) = best_v;
+      slot += k.count;
     }
-    P.tuning.m2l_variant = best_v;
     P.prof.on = prof;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -306,6 +372,38 @@ int mlfma_fgmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_
     if (history)
       for (int i = 0; i < history_cap && i < static_cast<int>(hist.size()); ++i) history[i] = hist[i];
     return ok ? MLFMA_OK : MLFMA_ERR_NOT_CONVERGED;
+  });
+}
+
+int mlfma_fgmres_batch(mlfma_plan* plan, int n, int R, double* x, const double* rhs, int itr_max, int mr,
+                       double tol_abs, double tol_rel, int inner_its, mlfma_solve_stats* stats) {
+  if (!plan || !plan->p || !x || !rhs) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (R <= 0) return fail(MLFMA_ERR_ARG, "R must be positive");
+  if (mr <= 0 || mr > 63 || itr_max < 0 || inner_its < 0 || inner_its > 63)
+    return fail(MLFMA_ERR_ARG, "need 1 <= mr <= 63, 0 <= inner_its <= 63, itr_max >= 0");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    std::vector<mlfma::SolveStats> st;
+    std::vector<std::vector<double>> hist;
+    double seconds = 0.0;
+    const std::vector<char> ok =
+        mlfma::fgmres_batch_solve(*plan->p, R, x, rhs, itr_max, mr, tol_abs, tol_rel, inner_its, st, hist, seconds);
+    bool all = true;
+    for (int q = 0; q < R; ++q) {
+      all = all && ok[q];
+      if (stats) {
+        stats[q].iterations = st[q].iterations;
+        stats[q].restarts = st[q].restarts;
+        stats[q].matvecs = st[q].matvecs;
+        stats[q].converged = ok[q] ? 1 : 0;
+        stats[q].rel_residual = st[q].rel_residual;
+        stats[q].seconds = st[q].seconds;
+        stats[q].history_len = 0;
+        stats[q].near_products = st[q].near_products;
+      }
+    }
+    return all ? MLFMA_OK : MLFMA_ERR_NOT_CONVERGED;
   });
 }
 

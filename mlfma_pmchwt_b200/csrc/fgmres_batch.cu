@@ -1,0 +1,564 @@
+// Lockstep multi-right-hand-side FGMRES: R independent systems A x_q = b_q
+// (one per plane-wave incidence, say) iterate together, so each Arnoldi
+// step costs one batched operator apply (leaf patterns and near-field
+// entries read once per group of right-hand sides, matvec_kernels.cu) and
+// one batched near-field product per inner step, and every Gram-Schmidt /
+// update step is one launch over all active systems with one host sync.
+// Per system the iteration is exactly fgmres_solve's (fgmres.cu): the
+// reference's restarted GMRES (Code/GMRES.h:65-217) with CGS2 Arnoldi,
+// complex Givens rotations, true residual per cycle and its divergence
+// abort, optionally right-preconditioned by inner GMRES steps on Z_near.
+// A system leaves the lockstep set when it converges, breaks down or runs
+// out of iterations; the others go on.
+#include <algorithm>
+#include <chrono>
+#include <complex>
+#include <vector>
+
+#include "blas1.cuh"
+#include "cplx.cuh"
+#include "plan.hpp"
+#include "solver.hpp"
+
+namespace mlfma {
+
+namespace {
+
+using C = std::complex<double>;
+constexpr int kBT = 256;  // threads per block of the batched vector kernels
+
+// One operand of a batched kernel: the vector of lockstep position a lives at
+// p + (by_sys ? sys[a] : a) * stride + off.
+struct VecRef {
+  double2* p;
+  long long stride, off;
+  int by_sys;
+  __device__ __forceinline__ double2* at(int a, const int* sys) const {
+    return p + (by_sys ? sys[a] : a) * stride + off;
+  }
+};
+
+__device__ __forceinline__ double2 bsum(double2 v, double2* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < (blockDim.x >> 5) ? sh[lane] : c2(0.0, 0.0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+      v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+  }
+  return v;
+}
+
+// part[(a * nblk + blk) * ldp + j] = block partial of conj(V_j) . w, j < nv
+// (V_j = basis vector j of the operand V: stride between basis vectors n)
+__global__ void __launch_bounds__(kBT) dots_b(VecRef V, VecRef w, const int* sys, long long n, int nv,
+                                             double2* part, int ldp) {
+  __shared__ double2 sh[kBT / 32];
+  const int a = blockIdx.y, nblk = gridDim.x;
+  const double2* Vb = V.at(a, sys);
+  const double2* wb = w.at(a, sys);
+  for (int j0 = 0; j0 < nv; j0 += blas1::kTile) {
+    double2 acc[blas1::kTile];
+#pragma unroll
+    for (int q = 0; q < blas1::kTile; ++q) acc[q] = c2(0.0, 0.0);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)nblk * blockDim.x) {
+      const double2 wi = wb[i];
+#pragma unroll
+      for (int q = 0; q < blas1::kTile; ++q)
+        if (j0 + q < nv) {
+          const double2 v = Vb[(long long)(j0 + q) * n + i];
+          acc[q].x = fma(v.x, wi.x, fma(v.y, wi.y, acc[q].x));
+          acc[q].y = fma(v.x, wi.y, fma(-v.y, wi.x, acc[q].y));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < blas1::kTile; ++q)
+      if (j0 + q < nv) {
+        const double2 s = bsum(acc[q], sh);
+        if (threadIdx.x == 0) part[((long long)a * nblk + blockIdx.x) * ldp + j0 + q] = s;
+      }
+  }
+}
+
+// out[a * ldo + j] = sum over blocks, j < nv; grid.y = positions
+__global__ void reduce_b(const double2* part, int nblk, int ldp, int nv, double2* out, int ldo) {
+  const int a = blockIdx.y;
+  for (int j = threadIdx.x; j < nv; j += blockDim.x) {
+    double2 s = c2(0.0, 0.0);
+    for (int b = 0; b < nblk; ++b) s = cadd(s, part[((long long)a * nblk + b) * ldp + j]);
+    out[(long long)a * ldo + j] = s;
+  }
+}
+
+// w -= sum_j V_j h[a * ldh + j]; with want_norm the block partials of ||w||^2
+// into part[(a * nblk + blk) * ldp]
+__global__ void __launch_bounds__(kBT) project_b(VecRef V, VecRef w, const int* sys, long long n, int nv,
+                                                const double2* h, int ldh, int want_norm, double2* part,
+                                                int ldp) {
+  __shared__ double2 hs[blas1::kMaxBasis];
+  __shared__ double2 sh[kBT / 32];
+  const int a = blockIdx.y, nblk = gridDim.x;
+  const double2* Vb = V.at(a, sys);
+  double2* wb = w.at(a, sys);
+  for (int j = threadIdx.x; j < nv; j += blockDim.x) hs[j] = h[(long long)a * ldh + j];
+  __syncthreads();
+  double2 nrm = c2(0.0, 0.0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)nblk * blockDim.x) {
+    double2 wi = wb[i];
+    for (int j = 0; j < nv; ++j) wi = csub(wi, cmul(hs[j], Vb[(long long)j * n + i]));
+    wb[i] = wi;
+    nrm.x = fma(wi.x, wi.x, fma(wi.y, wi.y, nrm.x));
+  }
+  if (want_norm) {
+    const double2 s = bsum(nrm, sh);
+    if (threadIdx.x == 0) part[((long long)a * nblk + blockIdx.x) * ldp] = s;
+  }
+}
+
+// block partials of ||w||^2, or of ||b - w||^2 with r = b - w written (has_b)
+__global__ void __launch_bounds__(kBT) norm_b(VecRef b, VecRef w, VecRef r, const int* sys, long long n, int has_b,
+                                             double2* part, int ldp) {
+  __shared__ double2 sh[kBT / 32];
+  const int a = blockIdx.y, nblk = gridDim.x;
+  const double2* wb = w.at(a, sys);
+  const double2* bb = has_b ? b.at(a, sys) : nullptr;
+  double2* rb = has_b ? r.at(a, sys) : nullptr;
+  double2 nrm = c2(0.0, 0.0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)nblk * blockDim.x) {
+    double2 v = wb[i];
+    if (has_b) {
+      v = csub(bb[i], v);
+      rb[i] = v;
+    }
+    nrm.x = fma(v.x, v.x, fma(v.y, v.y, nrm.x));
+  }
+  const double2 s = bsum(nrm, sh);
+  if (threadIdx.x == 0) part[((long long)a * nblk + blockIdx.x) * ldp] = s;
+}
+
+// dst = alpha[a] * src
+__global__ void scale_b(VecRef src, VecRef dst, const int* sys, long long n, const double* alpha) {
+  const int a = blockIdx.y;
+  const double2* s = src.at(a, sys);
+  double2* d = dst.at(a, sys);
+  const double al = alpha[a];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    d[i] = cscale(s[i], al);
+}
+
+// x (+)= sum_{j < m[a]} V_j y[a * ldy + j]
+__global__ void combine_b(VecRef V, VecRef x, const int* sys, long long n, const int* m, const double2* y, int ldy,
+                          int accumulate) {
+  __shared__ double2 ys[blas1::kMaxBasis];
+  const int a = blockIdx.y;
+  const int ma = m[a];
+  const double2* Vb = V.at(a, sys);
+  double2* xb = x.at(a, sys);
+  for (int j = threadIdx.x; j < ma; j += blockDim.x) ys[j] = y[(long long)a * ldy + j];
+  __syncthreads();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double2 xi = accumulate ? xb[i] : c2(0.0, 0.0);
+    for (int j = 0; j < ma; ++j) xi = cfma(ys[j], Vb[(long long)j * n + i], xi);
+    xb[i] = xi;
+  }
+}
+
+// dst = src (gather into / scatter out of the contiguous staging block)
+__global__ void copy_b(VecRef src, VecRef dst, const int* sys, long long n) {
+  const int a = blockIdx.y;
+  const double2* s = src.at(a, sys);
+  double2* d = dst.at(a, sys);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    d[i] = s[i];
+}
+
+// w_a = Z_near x_a for every position (warp per RWG, 4 right-hand sides per
+// warp): the near-field rows of the plan, read once per group of four.
+struct NearBatchArg {
+  const int* leaf_rwg;
+  const int* rwg_box;
+  const int* leaf_ptr;
+  const int* near_sptr;
+  const int* near_src;
+  const long long* near_zoff;
+  const double2* near_z;
+  VecRef x, w;
+  const int* sys;
+  int N, R;
+};
+
+constexpr int kNearRB = 4;
+
+__global__ void __launch_bounds__(128) near_batch_kernel(NearBatchArg a) {
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (r >= a.N) return;
+  const int p0 = blockIdx.y * kNearRB, pn = min(kNearRB, a.R - p0);
+  const int id = a.leaf_rwg[r];
+  const int b = a.rwg_box[id];
+  const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
+  const int tl = r - a.leaf_ptr[b];
+  const double2* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
+  double2 nJ[kNearRB], nM[kNearRB];
+  const double2* xs[kNearRB];
+#pragma unroll
+  for (int j = 0; j < kNearRB; ++j) {
+    nJ[j] = nM[j] = c2(0.0, 0.0);
+    xs[j] = j < pn ? a.x.at(p0 + j, a.sys) : nullptr;
+  }
+  for (int q = lane; q < ns; q += 32) {
+    const int src = a.near_src[s0 + q];
+    const double2 z11 = Z[3 * q], z12 = Z[3 * q + 1], z22 = Z[3 * q + 2];
+#pragma unroll
+    for (int j = 0; j < kNearRB; ++j) {
+      if (j < pn) {
+        const double2 xJ = xs[j][src], xM = xs[j][a.N + src];
+        nJ[j] = cfma(z11, xJ, cfma(z12, xM, nJ[j]));
+        nM[j] = cfma(z22, xM, csub(nM[j], cmul(z12, xJ)));
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kNearRB; ++j) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      nJ[j].x += __shfl_xor_sync(0xffffffffu, nJ[j].x, o);
+      nJ[j].y += __shfl_xor_sync(0xffffffffu, nJ[j].y, o);
+      nM[j].x += __shfl_xor_sync(0xffffffffu, nM[j].x, o);
+      nM[j].y += __shfl_xor_sync(0xffffffffu, nM[j].y, o);
+    }
+    if (lane == 0 && j < pn) {
+      double2* w = a.w.at(p0 + j, a.sys);
+      w[id] = nJ[j];
+      w[a.N + id] = nM[j];
+    }
+  }
+}
+
+// Upper-triangular solve of the rotated least-squares system (Code/GMRES.h:165-182).
+void back_substitute(const std::vector<C>& H, int ld, const std::vector<C>& s, int m, std::vector<C>& y) {
+  const double eps = 1e-16;
+  y.assign(m, C(0.0));
+  for (int i = m - 1; i >= 0; --i) {
+    y[i] = s[i];
+    for (int j = i + 1; j < m; ++j) y[i] -= H[i + j * ld] * y[j];
+    if (std::abs(H[i + i * ld]) > eps)
+      y[i] /= H[i + i * ld];
+    else
+      y[i] = C(0.0);
+  }
+}
+
+// Host side of the batched vector steps on one stream, for up to R positions.
+struct BatchOps {
+  cudaStream_t s;
+  long long n;
+  int nblk;          // blocks per system
+  int ldp;           // partial row length
+  double2* part;     // [R][nblk][ldp]
+  double2* hdev;     // [R][2 * ldp + 2]
+  double* alpha;     // [R]
+  int* mdev;         // [R]
+  double2* ydev;     // [R][kMaxBasis]
+  std::vector<C> hbuf;
+
+  dim3 grid(int Ra) const { return dim3(nblk, Ra); }
+
+  // norms of the operand (or of b - w, writing r) for Ra positions
+  std::vector<double> norms(int Ra, const int* sys, VecRef w, VecRef b = {}, VecRef r = {}, bool has_b = false) {
+    norm_b<<<grid(Ra), kBT, 0, s>>>(b, w, r, sys, n, has_b ? 1 : 0, part, ldp);
+    reduce_b<<<dim3(1, Ra), 32, 0, s>>>(part, nblk, ldp, 1, hdev, 2 * ldp + 2);
+    hbuf.resize(static_cast<size_t>(Ra) * (2 * ldp + 2));
+    MLFMA_CUDA(cudaMemcpyAsync(hbuf.data(), hdev, hbuf.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    MLFMA_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> out(Ra);
+    for (int a = 0; a < Ra; ++a) out[a] = std::sqrt(hbuf[static_cast<size_t>(a) * (2 * ldp + 2)].real());
+    return out;
+  }
+  // CGS2 of w_a against V_a[0..nv): hcol[a][j] and ||w_a|| after projection
+  void orthogonalise(int Ra, const int* sys, VecRef V, VecRef w, int nv, std::vector<std::vector<C>>& hcol,
+                     std::vector<double>& hn) {
+    const int ldh = 2 * ldp + 2;
+    dots_b<<<grid(Ra), kBT, 0, s>>>(V, w, sys, n, nv, part, ldp);
+    reduce_b<<<dim3(1, Ra), 64, 0, s>>>(part, nblk, ldp, nv, hdev, ldh);
+    project_b<<<grid(Ra), kBT, 0, s>>>(V, w, sys, n, nv, hdev, ldh, 0, part, ldp);
+    dots_b<<<grid(Ra), kBT, 0, s>>>(V, w, sys, n, nv, part, ldp);
+    reduce_b<<<dim3(1, Ra), 64, 0, s>>>(part, nblk, ldp, nv, hdev + ldp, ldh);
+    project_b<<<grid(Ra), kBT, 0, s>>>(V, w, sys, n, nv, hdev + ldp, ldh, 1, part, ldp);
+    reduce_b<<<dim3(1, Ra), 32, 0, s>>>(part, nblk, ldp, 1, hdev + 2 * ldp, ldh);
+    hbuf.resize(static_cast<size_t>(Ra) * ldh);
+    MLFMA_CUDA(cudaMemcpyAsync(hbuf.data(), hdev, hbuf.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    MLFMA_CUDA(cudaStreamSynchronize(s));
+    hcol.assign(Ra, std::vector<C>(nv));
+    hn.assign(Ra, 0.0);
+    for (int a = 0; a < Ra; ++a) {
+      const C* h = hbuf.data() + static_cast<size_t>(a) * ldh;
+      for (int j = 0; j < nv; ++j) hcol[a][j] = h[j] + h[ldp + j];
+      hn[a] = std::sqrt(h[2 * ldp].real());
+    }
+  }
+  void scale(int Ra, const int* sys, VecRef src, VecRef dst, const std::vector<double>& al) {
+    MLFMA_CUDA(cudaMemcpyAsync(alpha, al.data(), Ra * sizeof(double), cudaMemcpyHostToDevice, s));
+    scale_b<<<grid(Ra), kBT, 0, s>>>(src, dst, sys, n, alpha);
+  }
+  void combine(int Ra, const int* sys, VecRef V, VecRef x, const std::vector<std::vector<C>>& y, bool acc) {
+    std::vector<int> m(Ra);
+    std::vector<C> yy(static_cast<size_t>(Ra) * blas1::kMaxBasis, C(0.0));
+    for (int a = 0; a < Ra; ++a) {
+      m[a] = static_cast<int>(y[a].size());
+      std::copy(y[a].begin(), y[a].end(), yy.begin() + static_cast<size_t>(a) * blas1::kMaxBasis);
+    }
+    MLFMA_CUDA(cudaMemcpyAsync(mdev, m.data(), Ra * sizeof(int), cudaMemcpyHostToDevice, s));
+    MLFMA_CUDA(cudaMemcpyAsync(ydev, yy.data(), yy.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+    combine_b<<<grid(Ra), kBT, 0, s>>>(V, x, sys, n, mdev, ydev, blas1::kMaxBasis, acc ? 1 : 0);
+  }
+  void copy(int Ra, const int* sys, VecRef src, VecRef dst) { copy_b<<<grid(Ra), kBT, 0, s>>>(src, dst, sys, n); }
+};
+
+}  // namespace
+
+std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* rhs, int itr_max, int mr, double tol_abs,
+                        double tol_rel, int inner_its, std::vector<SolveStats>& st,
+                        std::vector<std::vector<double>>& hist, double& seconds) {
+  if (R < 1) throw std::invalid_argument("R must be positive");
+  if (mr < 1 || mr + 1 > blas1::kMaxBasis) throw std::invalid_argument("mr must be in 1..63");
+  if (inner_its < 0 || inner_its + 1 > blas1::kMaxBasis) throw std::invalid_argument("inner_its must be in 0..63");
+  const auto t0 = std::chrono::steady_clock::now();
+  MLFMA_CUDA(cudaSetDevice(P.device));
+  reserve_batch(P, R);
+  cudaStream_t s = P.stream;
+  const long long n = 2LL * P.N;
+  blas1::Work g;
+  const int ldp = blas1::kMaxBasis + 2;
+  const long long vs = static_cast<long long>(mr + 1) * n;       // per-system basis stride
+  const long long zs = static_cast<long long>(mr) * n;
+  const long long qs = static_cast<long long>(inner_its + 1) * n;
+  double2* x = g.get(static_cast<size_t>(R) * n);
+  double2* b = g.get(static_cast<size_t>(R) * n);
+  double2* r = g.get(static_cast<size_t>(R) * n);
+  double2* V = g.get(static_cast<size_t>(R) * vs);
+  double2* Zd = inner_its > 0 ? g.get(static_cast<size_t>(R) * zs) : nullptr;
+  double2* Q = inner_its > 0 ? g.get(static_cast<size_t>(R) * qs) : nullptr;
+  const int G = std::min(R, kBatchSlots);  // staging rows: one batched apply at a time
+  double2* Xs = g.get(static_cast<size_t>(G) * n);
+  double2* Ws = g.get(static_cast<size_t>(G) * n);
+  const int nblk = std::max(1, blas1::kBlocks / std::min(R, 8));
+  BatchOps ops{s, n, nblk, ldp};
+  ops.part = g.get(static_cast<size_t>(R) * nblk * ldp);
+  ops.hdev = g.get(static_cast<size_t>(R) * (2 * ldp + 2));
+  void* tmp = nullptr;
+  MLFMA_CUDA(cudaMalloc(&tmp, static_cast<size_t>(R) * sizeof(double)));
+  g.owned.push_back(tmp);
+  ops.alpha = static_cast<double*>(tmp);
+  MLFMA_CUDA(cudaMalloc(&tmp, static_cast<size_t>(R) * sizeof(int)));
+  g.owned.push_back(tmp);
+  ops.mdev = static_cast<int*>(tmp);
+  ops.ydev = g.get(static_cast<size_t>(R) * blas1::kMaxBasis);
+  MLFMA_CUDA(cudaMalloc(&tmp, static_cast<size_t>(R) * sizeof(int)));
+  g.owned.push_back(tmp);
+  int* sysd = static_cast<int*>(tmp);
+  MLFMA_CUDA(cudaMemcpyAsync(x, xh, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyHostToDevice, s));
+  MLFMA_CUDA(cudaMemcpyAsync(b, rhs, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyHostToDevice, s));
+  st.assign(R, SolveStats());
+  hist.assign(R, {});
+
+  auto set_sys = [&](const std::vector<int>& list) {
+    MLFMA_CUDA(cudaMemcpyAsync(sysd, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  };
+  auto sysref = [](double2* p, long long stride, long long off) { return VecRef{p, stride, off, 1}; };
+  auto posref = [&](double2* p) { return VecRef{p, n, 0, 0}; };
+  // out_q (offset off within its system block of stride stride) = A in_q,
+  // in groups of G through the staging rows; list = systems
+  auto batched_apply = [&](const std::vector<int>& list, VecRef in, VecRef out) {
+    for (size_t g0 = 0; g0 < list.size(); g0 += G) {
+      const int rn = static_cast<int>(std::min<size_t>(G, list.size() - g0));
+      std::vector<int> part(list.begin() + g0, list.begin() + g0 + rn);
+      set_sys(part);
+      ops.copy(rn, sysd, in, posref(Xs));
+      apply_batch_device(P, rn, Xs, n, Ws, n, s);
+      ops.copy(rn, sysd, posref(Ws), out);
+      for (int q : part) st[q].matvecs++;
+    }
+  };
+  // true residuals r_q = b_q - A x_q, returns ||r_q|| per listed system
+  auto true_residuals = [&](const std::vector<int>& list) {
+    batched_apply(list, sysref(x, n, 0), sysref(r, n, 0));
+    set_sys(list);
+    const int Ra = static_cast<int>(list.size());
+    // r holds A x: r = b - r in place
+    return ops.norms(Ra, sysd, sysref(r, n, 0), sysref(b, n, 0), sysref(r, n, 0), true);
+  };
+  // z_q = (inner_its GMRES steps on Z_near from zero) applied to v_q, q in list
+  auto precondition = [&](const std::vector<int>& list, long long voff, long long zoff) {
+    const int Ra = static_cast<int>(list.size());
+    set_sys(list);
+    const std::vector<double> beta = ops.norms(Ra, sysd, sysref(V, vs, voff));
+    std::vector<double> inv(Ra);
+    for (int a = 0; a < Ra; ++a) inv[a] = beta[a] > 0 ? 1.0 / beta[a] : 0.0;
+    ops.scale(Ra, sysd, sysref(V, vs, voff), sysref(Q, qs, 0), inv);
+    const int ld = inner_its + 1;
+    std::vector<std::vector<C>> Hi(Ra, std::vector<C>(static_cast<size_t>(ld) * inner_its, C(0.0)));
+    std::vector<std::vector<C>> ci(Ra, std::vector<C>(ld)), si(Ra, std::vector<C>(ld)), gi(Ra, std::vector<C>(ld));
+    std::vector<int> used(Ra, 0);
+    std::vector<char> done(Ra, 0);
+    for (int a = 0; a < Ra; ++a) gi[a][0] = beta[a];
+    std::vector<std::vector<C>> hcol;
+    std::vector<double> hn;
+    for (int j = 0; j < inner_its; ++j) {
+      NearBatchArg na{P.d_leaf_rwg, P.d_rwg_leafbox, P.d_leaf_ptr, P.d_near_sptr, P.d_near_src, P.d_near_zoff,
+                      P.d_near_z,   sysref(Q, qs, j * n), sysref(Q, qs, (j + 1) * n), sysd, P.N, Ra};
+      near_batch_kernel<<<dim3((P.N + 3) / 4, (Ra + kNearRB - 1) / kNearRB), 128, 0, s>>>(na);
+      MLFMA_CUDA(cudaGetLastError());
+      for (int q : list) st[q].near_products++;
+      ops.orthogonalise(Ra, sysd, sysref(Q, qs, 0), sysref(Q, qs, (j + 1) * n), j + 1, hcol, hn);
+      std::vector<double> sc(Ra, 1.0);
+      for (int a = 0; a < Ra; ++a) {
+        if (done[a]) continue;
+        std::vector<C>& H = Hi[a];
+        for (int i = 0; i <= j; ++i) H[i + j * ld] = hcol[a][i];
+        H[j + 1 + j * ld] = hn[a];
+        used[a] = j + 1;
+        if (hn[a] < 1e-14 * beta[a]) {
+          done[a] = 1;
+          continue;
+        }
+        sc[a] = 1.0 / hn[a];
+        for (int i = 0; i < j; ++i) blas1::givens_apply(H[i + j * ld], H[i + 1 + j * ld], ci[a][i], si[a][i]);
+        blas1::givens_make(H[j + j * ld], H[j + 1 + j * ld], ci[a][j], si[a][j]);
+        blas1::givens_apply(H[j + j * ld], H[j + 1 + j * ld], ci[a][j], si[a][j]);
+        H[j + 1 + j * ld] = C(0.0);
+        blas1::givens_apply(gi[a][j], gi[a][j + 1], ci[a][j], si[a][j]);
+      }
+      ops.scale(Ra, sysd, sysref(Q, qs, (j + 1) * n), sysref(Q, qs, (j + 1) * n), sc);
+    }
+    std::vector<std::vector<C>> y(Ra);
+    for (int a = 0; a < Ra; ++a) back_substitute(Hi[a], ld, gi[a], used[a], y[a]);
+    ops.combine(Ra, sysd, sysref(Q, qs, 0), sysref(Zd, zs, zoff), y, false);
+  };
+
+  const double eps = 1e-16;
+  std::vector<int> all(R);
+  for (int q = 0; q < R; ++q) all[q] = q;
+  std::vector<double> rnorm = true_residuals(all);
+  set_sys(all);
+  std::vector<double> bnorm = ops.norms(R, sysd, sysref(b, n, 0));
+  std::vector<double> error(R);
+  std::vector<char> conv(R, 0);
+  std::vector<int> live, total(R, 0);
+  for (int q = 0; q < R; ++q) {
+    if (bnorm[q] < eps) bnorm[q] = 1.0;
+    error[q] = rnorm[q] / bnorm[q];
+    st[q].rel_residual = error[q];
+    if (error[q] < tol_rel || error[q] < tol_abs)
+      conv[q] = 1;
+    else
+      live.push_back(q);
+  }
+  const int ld = mr + 1;
+  std::vector<std::vector<C>> H(R), cs(R), sn(R), sv(R);
+  std::vector<int> k_used(R, 0);
+  for (int cycle = 1; !live.empty(); ++cycle) {
+    // start of a cycle for every live system
+    set_sys(live);
+    {
+      std::vector<double> inv(live.size());
+      for (size_t a = 0; a < live.size(); ++a) inv[a] = 1.0 / rnorm[live[a]];
+      ops.scale(static_cast<int>(live.size()), sysd, sysref(r, n, 0), sysref(V, vs, 0), inv);
+    }
+    for (int q : live) {
+      st[q].restarts = cycle;
+      H[q].assign(static_cast<size_t>(ld) * mr, C(0.0));
+      cs[q].assign(mr, C(0.0));
+      sn[q].assign(mr, C(0.0));
+      sv[q].assign(mr + 1, C(0.0));
+      sv[q][0] = rnorm[q];
+      k_used[q] = 0;
+    }
+    std::vector<int> act = live;  // systems still stepping in this cycle
+    for (int k = 0; k < mr && !act.empty(); ++k) {
+      std::vector<int> step;
+      for (int q : act)
+        if (total[q] < itr_max) step.push_back(q);
+      if (step.empty()) break;
+      for (int q : step) {
+        ++total[q];
+        k_used[q] = k + 1;
+      }
+      VecRef zk = inner_its > 0 ? sysref(Zd, zs, k * n) : sysref(V, vs, k * n);
+      if (inner_its > 0) precondition(step, k * n, k * n);
+      // w_q = A z_q into the next basis slot, then CGS2 against V_q[0..k]
+      batched_apply(step, zk, sysref(V, vs, (k + 1) * n));
+      set_sys(step);
+      const int Ra = static_cast<int>(step.size());
+      std::vector<std::vector<C>> hcol;
+      std::vector<double> hn;
+      ops.orthogonalise(Ra, sysd, sysref(V, vs, 0), sysref(V, vs, (k + 1) * n), k + 1, hcol, hn);
+      std::vector<double> sc(Ra, 1.0);
+      std::vector<int> next;
+      for (int a = 0; a < Ra; ++a) {
+        const int q = step[a];
+        std::vector<C>& Hq = H[q];
+        for (int j = 0; j <= k; ++j) Hq[j + static_cast<size_t>(k) * ld] = hcol[a][j];
+        Hq[k + 1 + static_cast<size_t>(k) * ld] = hn[a];
+        if (hn[a] < eps * rnorm[q]) continue;  // breakdown: this cycle ends for q
+        sc[a] = 1.0 / hn[a];
+        for (int j = 0; j < k; ++j) blas1::givens_apply(Hq[j + k * ld], Hq[j + 1 + k * ld], cs[q][j], sn[q][j]);
+        blas1::givens_make(Hq[k + k * ld], Hq[k + 1 + k * ld], cs[q][k], sn[q][k]);
+        blas1::givens_apply(Hq[k + k * ld], Hq[k + 1 + k * ld], cs[q][k], sn[q][k]);
+        Hq[k + 1 + k * ld] = C(0.0);
+        blas1::givens_apply(sv[q][k], sv[q][k + 1], cs[q][k], sn[q][k]);
+        error[q] = std::abs(sv[q][k + 1]) / bnorm[q];
+        hist[q].push_back(error[q]);
+        if (!(error[q] < tol_rel || error[q] < tol_abs)) next.push_back(q);
+      }
+      ops.scale(Ra, sysd, sysref(V, vs, (k + 1) * n), sysref(V, vs, (k + 1) * n), sc);
+      act = next;
+    }
+    // update x_q with the cycle's least-squares solution, then true residuals
+    set_sys(live);
+    std::vector<std::vector<C>> y(live.size());
+    for (size_t a = 0; a < live.size(); ++a) {
+      const int q = live[a];
+      back_substitute(H[q], ld, sv[q], std::min(k_used[q], mr), y[a]);
+    }
+    ops.combine(static_cast<int>(live.size()), sysd, inner_its > 0 ? sysref(Zd, zs, 0) : sysref(V, vs, 0),
+                sysref(x, n, 0), y, true);
+    const std::vector<double> rn = true_residuals(live);
+    std::vector<int> keep;
+    for (size_t a = 0; a < live.size(); ++a) {
+      const int q = live[a];
+      rnorm[q] = rn[a];
+      error[q] = rn[a] / bnorm[q];
+      st[q].iterations = total[q];
+      st[q].rel_residual = error[q];
+      if (error[q] < tol_rel || error[q] < tol_abs) {
+        conv[q] = 1;
+        continue;
+      }
+      if (total[q] >= itr_max) continue;
+      if (error[q] > 100.0 * tol_rel && cycle > 8 && error[q] > 1000.0 * tol_rel) continue;  // divergence abort
+      keep.push_back(q);
+    }
+    live = keep;
+  }
+  MLFMA_CUDA(cudaMemcpyAsync(xh, x, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  MLFMA_CUDA(cudaStreamSynchronize(s));
+  seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  for (int q = 0; q < R; ++q) {
+    st[q].seconds = seconds;
+    if (!conv[q]) st[q].iterations = total[q];
+  }
+  return std::vector<char>(conv);
+}
+
+}  // namespace mlfma

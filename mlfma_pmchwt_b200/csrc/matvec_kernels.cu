@@ -13,6 +13,8 @@
 // Every stage writes its output before anything accumulates into it (l2l adds
 // onto the Bm that m2l of the same level has just written), so no clearing
 // pass (Code/ProcessMLFMM.h:14-28) is needed.
+#include <algorithm>
+
 #include "cplx.cuh"
 #include "plan.hpp"
 
@@ -47,6 +49,70 @@ __global__ void __launch_bounds__(kThreads) agg_kernel(const double2* __restrict
   double2* out = S + static_cast<size_t>(b) * 6 * K + kk;
 #pragma unroll
   for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * K] = acc[c];
+}
+
+struct AggBoxArg {
+  const double2* Vs[2];  // radiation patterns per medium [N][3][K] (leaf order)
+  double2* S[2];         // leaf-level patterns per medium [Bleaf][6][K]
+  int K[2];
+  const int* leaf_ptr;
+  const int* leaf_rwg;
+  const double2* x;
+  int N;
+};
+
+// Aggregation, CTA per (leaf box, medium): the box's radiation patterns are
+// one contiguous block [n_b][3K] in leaf order, streamed by threads over its
+// 3K entries, two columns per thread (J components land at S[b][0..2], M at
+// S[b][3..5]). The box's currents are staged in shared memory first (boxes
+// of more than kAggStage RWGs read them from global memory).
+constexpr int kAggStage = 64;
+
+__global__ void __launch_bounds__(kThreads) agg_box_kernel(AggBoxArg a) {
+  __shared__ double2 sx[2][kAggStage];
+  const int b = blockIdx.x, m = blockIdx.y;
+  const int K3 = 3 * a.K[m];
+  const int r0 = a.leaf_ptr[b], nb = a.leaf_ptr[b + 1] - r0;
+  const bool staged = nb <= kAggStage;
+  if (staged)
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+      const int id = a.leaf_rwg[r0 + i];
+      sx[0][i] = a.x[id];
+      sx[1][i] = a.x[a.N + id];
+    }
+  __syncthreads();
+  const double2* V = a.Vs[m] + static_cast<size_t>(r0) * K3;
+  double2* out = a.S[m] + static_cast<size_t>(b) * 2 * K3;
+  for (int e0 = threadIdx.x; e0 < K3; e0 += 2 * blockDim.x) {
+    const int e1 = e0 + blockDim.x;
+    const bool two = e1 < K3;
+    double2 aJ0 = c2(0.0, 0.0), aM0 = c2(0.0, 0.0), aJ1 = c2(0.0, 0.0), aM1 = c2(0.0, 0.0);
+    const double2* v = V + e0;
+#pragma unroll 4
+    for (int r = 0; r < nb; ++r, v += K3) {
+      double2 xJ, xM;
+      if (staged) {
+        xJ = sx[0][r];
+        xM = sx[1][r];
+      } else {
+        const int id = __ldg(a.leaf_rwg + r0 + r);
+        xJ = __ldg(a.x + id);
+        xM = __ldg(a.x + a.N + id);
+      }
+      const double2 s0 = __ldg(v);
+      const double2 s1 = two ? __ldg(v + blockDim.x) : c2(0.0, 0.0);
+      aJ0 = cfma(s0, xJ, aJ0);
+      aM0 = cfma(s0, xM, aM0);
+      aJ1 = cfma(s1, xJ, aJ1);
+      aM1 = cfma(s1, xM, aM1);
+    }
+    out[e0] = aJ0;
+    out[K3 + e0] = aM0;
+    if (two) {
+      out[e1] = aJ1;
+      out[K3 + e1] = aM1;
+    }
+  }
 }
 
 struct UpArg {
@@ -94,6 +160,73 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg a) {
     acc = cfma(e, v, acc);
   }
   a.Sp[(static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
+}
+
+struct UpSepArg {
+  const double2* Sc;   // child level patterns [Bc][6][Kc]
+  double2* Sp;         // parent level patterns [Bp][6][Kp]
+  const int* child_begin;
+  const int* octant;   // of child boxes
+  const int* pidx;     // [nphp][3] into the child phi grid
+  const double* lp;
+  const double* lt;    // [nthp][3]
+  const int* row_ptr;  // per band: child theta rows it needs
+  const int* row;
+  const int* tpos;     // [nthp][3]: band row of each theta tap
+  const double2* ph_up;
+  int nthp, nphp, nphc, Kc, R;
+};
+
+// Interpolation (m2m), separable: CTA per (parent box, component, band of R
+// parent theta rows). For each child, the phi interpolation of the child
+// rows the band needs goes to shared memory (3 taps), then each parent
+// direction takes its 3 theta taps from there, times the child's shift
+// phase, accumulated over the children in registers. The reference's 9-tap
+// weight is the product of the two 1-D weights (Code/AlgoMLFMM.h:347-351).
+__global__ void __launch_bounds__(256) up_sep_kernel(UpSepArg a) {
+  __shared__ double2 T[kUpBandEntries];
+  const int P = blockIdx.x, c = blockIdx.y, bi = blockIdx.z;
+  const int t0 = bi * a.R;
+  const int nout = min(a.R, a.nthp - t0) * a.nphp;
+  const int r0 = a.row_ptr[bi], nr = a.row_ptr[bi + 1] - r0;
+  const int Kp = a.nthp * a.nphp;
+  constexpr int kPer = kUpBandOut / 256;
+  double2 acc[kPer];
+#pragma unroll
+  for (int q = 0; q < kPer; ++q) acc[q] = c2(0.0, 0.0);
+  const int ch1 = a.child_begin[P + 1];
+  for (int ch = a.child_begin[P]; ch < ch1; ++ch) {
+    const double2* sc = a.Sc + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * a.nphp; e += blockDim.x) {
+      const int r = e / a.nphp, p = e - r * a.nphp;
+      const double2* srow = sc + __ldg(a.row + r0 + r) * a.nphc;
+      double2 v = cscale(__ldg(srow + __ldg(a.pidx + 3 * p)), __ldg(a.lp + 3 * p));
+      v = cfmas(__ldg(a.lp + 3 * p + 1), __ldg(srow + __ldg(a.pidx + 3 * p + 1)), v);
+      v = cfmas(__ldg(a.lp + 3 * p + 2), __ldg(srow + __ldg(a.pidx + 3 * p + 2)), v);
+      T[e] = v;
+    }
+    __syncthreads();
+    const double2* ph = a.ph_up + a.octant[ch] * Kp + t0 * a.nphp;
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      const int e = threadIdx.x + q * 256;
+      if (e < nout) {
+        const int r = e / a.nphp, p = e - r * a.nphp;
+        const int t = t0 + r;
+        double2 v = cscale(T[__ldg(a.tpos + 3 * t) * a.nphp + p], __ldg(a.lt + 3 * t));
+        v = cfmas(__ldg(a.lt + 3 * t + 1), T[__ldg(a.tpos + 3 * t + 1) * a.nphp + p], v);
+        v = cfmas(__ldg(a.lt + 3 * t + 2), T[__ldg(a.tpos + 3 * t + 2) * a.nphp + p], v);
+        acc[q] = cfma(__ldg(ph + e), v, acc[q]);
+      }
+    }
+  }
+  double2* out = a.Sp + (static_cast<size_t>(P) * 6 + c) * Kp + t0 * a.nphp;
+#pragma unroll
+  for (int q = 0; q < kPer; ++q) {
+    const int e = threadIdx.x + q * 256;
+    if (e < nout) out[e] = acc[q];
+  }
 }
 
 struct M2lArg {
@@ -209,6 +342,181 @@ __global__ void __launch_bounds__(kTileDirs * kTileWarps) m2l_tile_kernel(M2lTil
   }
 }
 
+// Translation by octant registers, all levels of one medium in one launch.
+// A CTA takes one parent box and 64 directions; thread (direction, half,
+// group) keeps the incoming patterns of 4 of the parent's 8 octant children
+// (group 0: octants 0-3, group 1: 4-7) for the J (half 0) or M (half 1)
+// components in registers. The union of the children's interaction-list
+// sources is staged in shared memory; each source pattern is loaded once per
+// thread (the next one prefetched) and applied to every child of the group
+// whose list holds it (octant mask), with that child's transfer factor.
+constexpr int kM2lDirs = 64;
+constexpr int kM2lThreads = 4 * kM2lDirs;
+constexpr int kM2lMaxSeg = 14;  // levels 2..15
+constexpr int kM2lStage = 512;  // union entries staged per round
+
+struct M2lSeg {
+  const double2* S;
+  double2* Bm;
+  const double2* tfw;
+  const int* off2vec;
+  const int* ufar_ptr;
+  const int* ufar;
+  const int* upack;
+  const int* child_begin;  // parent level
+  const int* octant;       // this level
+  int K, nchunk, cta_begin;
+};
+struct M2lOctArg {
+  M2lSeg seg[kM2lMaxSeg];
+  int nseg;
+};
+
+__global__ void __launch_bounds__(kM2lThreads, 2) m2l_oct_kernel(const __grid_constant__ M2lOctArg a) {
+  __shared__ int sVec[343];
+  __shared__ int sChild[8];
+  __shared__ int sSrc[kM2lStage];
+  __shared__ int sPack[kM2lStage];
+  int si = 0;
+  while (si + 1 < a.nseg && static_cast<int>(blockIdx.x) >= a.seg[si + 1].cta_begin) ++si;
+  const M2lSeg& g = a.seg[si];
+  const int local = blockIdx.x - g.cta_begin;
+  const int P = local / g.nchunk;
+  const int k = (local - P * g.nchunk) * kM2lDirs + (threadIdx.x & (kM2lDirs - 1));
+  const int h = (threadIdx.x / kM2lDirs) & 1;   // J or M
+  const int grp = threadIdx.x / (2 * kM2lDirs);  // octants 4 grp .. 4 grp + 3
+  const int K = g.K;
+  const bool live = k < K;
+  const int kq = live ? k : K - 1;
+  for (int i = threadIdx.x; i < 343; i += blockDim.x) sVec[i] = g.off2vec[i];
+  if (threadIdx.x < 8) sChild[threadIdx.x] = -1;
+  __syncthreads();
+  const int c0 = g.child_begin[P], c1 = g.child_begin[P + 1];
+  if (threadIdx.x < c1 - c0) sChild[g.octant[c0 + threadIdx.x]] = c0 + threadIdx.x;
+  double2 acc[4][3];
+#pragma unroll
+  for (int o = 0; o < 4; ++o)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[o][c] = c2(0.0, 0.0);
+  const double2* Sbase = g.S + static_cast<size_t>(3 * h) * K + kq;
+  const int u0 = g.ufar_ptr[P], nu = g.ufar_ptr[P + 1] - u0;
+  for (int base = 0; base < nu; base += kM2lStage) {
+    const int nb = min(kM2lStage, nu - base);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+      sSrc[i] = g.ufar[u0 + base + i];
+      sPack[i] = g.upack[u0 + base + i];
+    }
+    __syncthreads();
+    const double2* src = Sbase + static_cast<size_t>(sSrc[0]) * 6 * K;
+    double2 n0 = __ldg(src), n1 = __ldg(src + K), n2 = __ldg(src + 2 * K);
+    for (int j = 0; j < nb; ++j) {
+      const double2 s0 = n0, s1 = n1, s2 = n2;
+      if (j + 1 < nb) {
+        src = Sbase + static_cast<size_t>(sSrc[j + 1]) * 6 * K;
+        n0 = __ldg(src);
+        n1 = __ldg(src + K);
+        n2 = __ldg(src + 2 * K);
+      }
+      const int pk = sPack[j];
+      const int enc0 = pk & 511;
+      const int mask = (pk >> (9 + 4 * grp)) & 15;
+      double2 tf[4];
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        const int oo = 4 * grp + o;
+        const int v = sVec[enc0 + (oo & 1) * 49 + ((oo >> 1) & 1) * 7 + (oo >> 2)];
+        tf[o] = (mask >> o) & 1 ? __ldg(g.tfw + static_cast<size_t>(max(v, 0)) * K + kq) : c2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        if ((mask >> o) & 1) {
+          acc[o][0] = cfma(tf[o], s0, acc[o][0]);
+          acc[o][1] = cfma(tf[o], s1, acc[o][1]);
+          acc[o][2] = cfma(tf[o], s2, acc[o][2]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (!live) return;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    const int t = sChild[4 * grp + o];
+    if (t >= 0) {
+      double2* out = g.Bm + (static_cast<size_t>(t) * 6 + 3 * h) * K + k;
+      out[0] = acc[o][0];
+      out[static_cast<size_t>(K)] = acc[o][1];
+      out[2 * static_cast<size_t>(K)] = acc[o][2];
+    }
+  }
+}
+
+// Translation, warp per box: a CTA takes 8 Morton-consecutive boxes (one
+// warp each) and 32 directions; every level of a medium in one launch. Each
+// lane accumulates its box's 6 components over the box's interaction list,
+// with one transfer-factor load per entry. Neighbouring boxes' lists hold
+// largely the same sources in the same (ascending) order, so the 8 warps
+// read the same source patterns at about the same time and L1 serves the
+// repeats.
+constexpr int kWarpBoxes = 8;
+
+struct M2lWarpSeg {
+  const double2* S;
+  double2* Bm;
+  const double2* tfw;
+  const int* far_ptr;
+  const int* far_idx;
+  const int* far_vec;
+  int B, K, nchunk, cta_begin;
+};
+struct M2lWarpArg {
+  M2lWarpSeg seg[kM2lMaxSeg];
+  int nseg;
+};
+
+__global__ void __launch_bounds__(32 * kWarpBoxes) m2l_warp_kernel(const __grid_constant__ M2lWarpArg a) {
+  int si = 0;
+  while (si + 1 < a.nseg && static_cast<int>(blockIdx.x) >= a.seg[si + 1].cta_begin) ++si;
+  const M2lWarpSeg& g = a.seg[si];
+  const int local = blockIdx.x - g.cta_begin;
+  const int grp = local / g.nchunk;
+  const int b = grp * kWarpBoxes + (threadIdx.x >> 5);
+  const int k = (local - grp * g.nchunk) * 32 + (threadIdx.x & 31);
+  const int K = g.K;
+  if (b >= g.B || k >= K) return;
+  double2 acc[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) acc[c] = c2(0.0, 0.0);
+  const int e1 = g.far_ptr[b + 1];
+  int e = g.far_ptr[b];
+  for (; e + 1 < e1; e += 2) {
+    const int s0 = __ldg(g.far_idx + e), s1 = __ldg(g.far_idx + e + 1);
+    const double2 t0 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e)) * K + k);
+    const double2 t1 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e + 1)) * K + k);
+    const double2* p0 = g.S + static_cast<size_t>(s0) * 6 * K + k;
+    const double2* p1 = g.S + static_cast<size_t>(s1) * 6 * K + k;
+    double2 v0[6], v1[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      v0[c] = __ldg(p0 + static_cast<size_t>(c) * K);
+      v1[c] = __ldg(p1 + static_cast<size_t>(c) * K);
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[c] = cfma(t1, v1[c], cfma(t0, v0[c], acc[c]));
+  }
+  if (e < e1) {
+    const int s0 = __ldg(g.far_idx + e);
+    const double2 t0 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e)) * K + k);
+    const double2* p0 = g.S + static_cast<size_t>(s0) * 6 * K + k;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[c] = cfma(t0, __ldg(p0 + static_cast<size_t>(c) * K), acc[c]);
+  }
+  double2* out = g.Bm + static_cast<size_t>(b) * 6 * K + k;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * K] = acc[c];
+}
+
 struct L2lArg {
   double2* Bm;           // child level (accumulated into)
   const double2* Bp;     // parent level
@@ -256,44 +564,59 @@ struct L2lSepArg {
   int ntc, npc, ntp, npp;
 };
 
-constexpr int kL2lRows = 8;        // child theta rows per band at most
-constexpr int kL2lBand = 2944;     // band entries in shared memory (46 KiB)
-constexpr int kL2lMaxPhi = kL2lBand;
+constexpr int kL2lBand = 2944;     // band entries in shared memory (46 KiB), all 6 components
 
-// Anterpolation (l2l), separable: the parent's incoming pattern is shifted to
-// the child centre, then spread onto the child grid by the transposed
-// theta interpolation (into a shared-memory band of child rows x parent phi
-// columns) and the transposed phi interpolation. One CTA per (child box,
-// component); the reference's 9-tap weight of a (parent, child) direction
-// pair is the product of the two 1-D weights used here (Code/AlgoMLFMM.h:347-351).
+// Anterpolation (l2l), separable: one CTA per child box does all 6
+// components. The parent's incoming pattern is shifted to the child centre
+// and spread onto the child grid by the transposed theta interpolation (into
+// a shared-memory band of child rows x parent phi columns x 6 components),
+// then by the transposed phi interpolation, and added to the child's Bm. The
+// reference's 9-tap weight of a (parent, child) direction pair is the
+// product of the two 1-D weights used here (Code/AlgoMLFMM.h:347-351).
 __global__ void __launch_bounds__(256) l2l_sep_kernel(L2lSepArg a) {
   __shared__ double2 band[kL2lBand];
-  const int b = blockIdx.x, c = blockIdx.y;
-  const int band_rows = max(1, min(kL2lRows, kL2lBand / a.npp));
+  const int b = blockIdx.x;
+  const int band_rows = max(1, min(a.ntc, kL2lBand / (6 * a.npp)));
   const int Kp = a.ntp * a.npp, Kc = a.ntc * a.npc;
   const double2* ph = a.ph_dn + a.octant[b] * Kp;
-  const double2* bp = a.Bp + (static_cast<size_t>(a.parent[b]) * 6 + c) * Kp;
-  double2* out = a.Bm + (static_cast<size_t>(b) * 6 + c) * Kc;
+  const double2* bp = a.Bp + static_cast<size_t>(a.parent[b]) * 6 * Kp;
+  double2* out = a.Bm + static_cast<size_t>(b) * 6 * Kc;
   for (int tc0 = 0; tc0 < a.ntc; tc0 += band_rows) {
     const int rows = min(band_rows, a.ntc - tc0);
+    const int stride = rows * a.npp;
     __syncthreads();
-    for (int e = threadIdx.x; e < rows * a.npp; e += blockDim.x) {
+    for (int e = threadIdx.x; e < stride; e += blockDim.x) {
       const int r = e / a.npp, pp = e - r * a.npp;
       const int tc = tc0 + r;
-      double2 v = c2(0.0, 0.0);
-      for (int q = a.th_ptr[tc]; q < a.th_ptr[tc + 1]; ++q) {
-        const int kp = a.th_src[q] * a.npp + pp;
-        v = cfmas(a.th_w[q], cmul(__ldg(ph + kp), __ldg(bp + kp)), v);
+      double2 v[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) v[c] = c2(0.0, 0.0);
+      const int q1 = __ldg(a.th_ptr + tc + 1);
+      for (int q = __ldg(a.th_ptr + tc); q < q1; ++q) {
+        const int kp = __ldg(a.th_src + q) * a.npp + pp;
+        const double2 f = cscale(__ldg(ph + kp), __ldg(a.th_w + q));
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[c] = cfma(f, __ldg(bp + static_cast<size_t>(c) * Kp + kp), v[c]);
       }
-      band[r * a.npp + pp] = v;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) band[c * stride + e] = v[c];
     }
     __syncthreads();
     for (int e = threadIdx.x; e < rows * a.npc; e += blockDim.x) {
       const int r = e / a.npc, pc = e - r * a.npc;
-      double2 v = c2(0.0, 0.0);
-      for (int q = a.ph_ptr[pc]; q < a.ph_ptr[pc + 1]; ++q) v = cfmas(a.ph_w[q], band[r * a.npp + a.ph_src[q]], v);
+      double2 v[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) v[c] = c2(0.0, 0.0);
+      const int q1 = __ldg(a.ph_ptr + pc + 1);
+      for (int q = __ldg(a.ph_ptr + pc); q < q1; ++q) {
+        const double w = __ldg(a.ph_w + q);
+        const int src = r * a.npp + __ldg(a.ph_src + q);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[c] = cfmas(w, band[c * stride + src], v[c]);
+      }
       double2* o = out + (tc0 + r) * a.npc + pc;
-      *o = cadd(*o, v);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) o[static_cast<size_t>(c) * Kc] = cadd(o[static_cast<size_t>(c) * Kc], v[c]);
     }
   }
 }
@@ -386,65 +709,323 @@ __global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg a) {
   }
 }
 
-}  // namespace
+// ---------------------------------------------------------------- batched
+// Several right-hand sides per pass over the leaf tables: the aggregation and
+// the leaf testing + near field read each radiation / receive pattern and
+// each near-field entry once for a group of right-hand sides. Accumulation
+// orders are those of agg_box_kernel and leaf_out_kernel, so each right-hand
+// side of a batch gets the single apply's result.
+struct AggBatchArg {
+  const double2* Vs[2];
+  double2* S[2][kBatchSlots];  // leaf-level S of each slot
+  int K[2];
+  const int* leaf_ptr;
+  const int* leaf_rwg;
+  const double2* X;            // right-hand side j at X + j * ldx
+  long long ldx;
+  int N, R;
+};
 
-void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
-  const int L = P.maxL;
-  cudaEvent_t* ev = nullptr;
-  if (P.prof.on) {
-    if (P.prof.used == P.prof.sets.size()) {
-      if (P.prof.sets.size() >= 4096) throw std::runtime_error("stage profiler: read it at least every 4096 applies");
-      std::array<cudaEvent_t, StageProfiler::kEvents> set{};
-      for (auto& e : set) MLFMA_CUDA(cudaEventCreate(&e));
-      P.prof.sets.push_back(set);
+template <int RB>
+__global__ void __launch_bounds__(kThreads) agg_batch_kernel(AggBatchArg a) {
+  const int b = blockIdx.x, m = blockIdx.y;
+  const int j0 = blockIdx.z * RB, jn = min(RB, a.R - j0);
+  const int K3 = 3 * a.K[m];
+  const int r0 = a.leaf_ptr[b], r1 = a.leaf_ptr[b + 1];
+  const double2* V = a.Vs[m] + static_cast<size_t>(r0) * K3;
+  for (int e = threadIdx.x; e < K3; e += blockDim.x) {
+    double2 aJ[RB], aM[RB];
+#pragma unroll
+    for (int j = 0; j < RB; ++j) aJ[j] = aM[j] = c2(0.0, 0.0);
+    const double2* v = V + e;
+    for (int r = r0; r < r1; ++r, v += K3) {
+      const int id = __ldg(a.leaf_rwg + r);
+      const double2 s = __ldg(v);
+#pragma unroll
+      for (int j = 0; j < RB; ++j) {
+        if (j < jn) {
+          const double2* x = a.X + (j0 + j) * a.ldx;
+          aJ[j] = cfma(s, __ldg(x + id), aJ[j]);
+          aM[j] = cfma(s, __ldg(x + a.N + id), aM[j]);
+        }
+      }
     }
-    ev = P.prof.sets[P.prof.used++].data();
-    MLFMA_CUDA(cudaEventRecord(ev[0], s));
+#pragma unroll
+    for (int j = 0; j < RB; ++j) {
+      if (j < jn) {
+        double2* out = a.S[m][j0 + j] + static_cast<size_t>(b) * 2 * K3;
+        out[e] = aJ[j];
+        out[K3 + e] = aM[j];
+      }
+    }
   }
+}
+
+struct LeafBatchArg {
+  const double2* Vf[2];
+  const double2* Bm[2][kBatchSlots];  // leaf-level Bm of each slot
+  const double* khat[2];
+  int K[2];
+  const int* leaf_rwg;
+  const int* rwg_box;
+  const int* leaf_ptr;
+  const int* near_sptr;
+  const int* near_src;
+  const long long* near_zoff;
+  const double2* near_z;
+  const double2* X;
+  long long ldx;
+  double2* W;
+  long long ldw;
+  int N, R;
+  double2 c1, c2, etai;
+};
+
+// One warp per (RWG, group of RB right-hand sides).
+template <int RB>
+__global__ void __launch_bounds__(kThreads) leaf_out_batch_kernel(LeafBatchArg a) {
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (r >= a.N) return;
+  const int j0 = blockIdx.y * RB, jn = min(RB, a.R - j0);
+  const int id = a.leaf_rwg[r];
+  const int b = a.rwg_box[id];
+  double2 wj[RB], wm[RB];
+#pragma unroll
   for (int m = 0; m < 2; ++m) {
-    const MediumLevel& leaf = P.ml[m][L];
-    dim3 g(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads);
-    agg_kernel<<<g, kThreads, 0, s>>>(P.d_Vs[m], P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, leaf.S);
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[1 + 4 * m], s));
-    for (int l = L - 1; l >= 2; --l) {
-      const MediumLevel& pm = P.ml[m][l];
-      const MediumLevel& cm = P.ml[m][l + 1];
-      UpArg a{cm.S, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
+    const int K = a.K[m];
+    const double2* V = a.Vf[m] + static_cast<size_t>(r) * 3 * K;
+    const double* kh = a.khat[m];
+    double2 acc[RB][4];  // LJ KJ LM KM
+#pragma unroll
+    for (int j = 0; j < RB; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[j][q] = c2(0.0, 0.0);
+    for (int kk = lane; kk < K; kk += 32) {
+      const double2 v0 = V[kk], v1 = V[K + kk], v2 = V[2 * K + kk];
+      // (-khat) x V
+      const double ax = -kh[kk], ay = -kh[K + kk], az = -kh[2 * K + kk];
+      const double2 w0 = csub(cscale(v2, ay), cscale(v1, az));
+      const double2 w1 = csub(cscale(v0, az), cscale(v2, ax));
+      const double2 w2 = csub(cscale(v1, ax), cscale(v0, ay));
+#pragma unroll
+      for (int j = 0; j < RB; ++j) {
+        if (j < jn) {
+          const double2* B = a.Bm[m][j0 + j] + static_cast<size_t>(b) * 6 * K;
+          const double2 b0 = B[kk], b1 = B[K + kk], b2 = B[2 * K + kk];
+          const double2 m0 = B[3 * K + kk], m1 = B[4 * K + kk], m2 = B[5 * K + kk];
+          acc[j][0] = cfma(v0, b0, cfma(v1, b1, cfma(v2, b2, acc[j][0])));
+          acc[j][2] = cfma(v0, m0, cfma(v1, m1, cfma(v2, m2, acc[j][2])));
+          acc[j][1] = cfma(w0, b0, cfma(w1, b1, cfma(w2, b2, acc[j][1])));
+          acc[j][3] = cfma(w0, m0, cfma(w1, m1, cfma(w2, m2, acc[j][3])));
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < RB; ++j) {
+      const double2 LJ = warp_sum(acc[j][0]), KJ = warp_sum(acc[j][1]);
+      const double2 LM = warp_sum(acc[j][2]), KM = warp_sum(acc[j][3]);
+      if (m == 0) {
+        wj[j] = cmul(a.c1, csub(LJ, KM));
+        wm[j] = cmul(a.c1, cadd(KJ, LM));
+      } else {
+        wj[j] = cadd(wj[j], cmul(a.c2, csub(cmul(a.etai, LJ), KM)));
+        wm[j] = cadd(wm[j], cmul(a.c2, cadd(KJ, cdiv(LM, a.etai))));
+      }
+    }
+  }
+  const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
+  const int tl = r - a.leaf_ptr[b];
+  const double2* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
+  double2 nJ[RB], nM[RB];
+#pragma unroll
+  for (int j = 0; j < RB; ++j) nJ[j] = nM[j] = c2(0.0, 0.0);
+  for (int q = lane; q < ns; q += 32) {
+    const int src = a.near_src[s0 + q];
+    const double2 z11 = Z[3 * q], z12 = Z[3 * q + 1], z22 = Z[3 * q + 2];
+#pragma unroll
+    for (int j = 0; j < RB; ++j) {
+      if (j < jn) {
+        const double2* x = a.X + (j0 + j) * a.ldx;
+        const double2 xJ = x[src], xM = x[a.N + src];
+        nJ[j] = cfma(z11, xJ, cfma(z12, xM, nJ[j]));
+        nM[j] = cfma(z22, xM, csub(nM[j], cmul(z12, xJ)));
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < RB; ++j) {
+    const double2 sJ = warp_sum(nJ[j]), sM = warp_sum(nM[j]);
+    if (lane == 0 && j < jn) {
+      double2* w = a.W + (j0 + j) * a.ldw;
+      w[id] = cadd(wj[j], sJ);
+      w[a.N + id] = cadd(wm[j], sM);
+    }
+  }
+}
+
+// Leaf-level pattern arrays of a tree pass: the plan's own, or one RHS slot
+// of a batched apply. Levels above the leaf always use the plan's arrays.
+struct LeafView {
+  const double2* S;
+  double2* B;
+};
+
+const double2* level_S(const Plan& P, int m, int l, const LeafView& v) { return l == P.maxL ? v.S : P.ml[m][l].S; }
+double2* level_B(const Plan& P, int m, int l, const LeafView& v) { return l == P.maxL ? v.B : P.ml[m][l].Bm; }
+
+// Interpolation up the tree (levels L-1 .. 2) of medium m.
+void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
+  const int L = P.maxL;
+  for (int l = L - 1; l >= 2; --l) {
+    const MediumLevel& pm = P.ml[m][l];
+    const MediumLevel& cm = P.ml[m][l + 1];
+    const double2* Sc = level_S(P, m, l + 1, v);
+    if (P.tuning.up_variant == 1 && pm.up_rows > 0) {
+      UpSepArg a{Sc,    pm.S,     P.lv[l].child_begin, P.lv[l + 1].octant, pm.pidx,
+                 pm.lp, pm.lt,    pm.up_row_ptr,       pm.up_row,          pm.up_tpos,
+                 pm.ph_up, pm.nth, pm.nph,             cm.nph,             cm.K,
+                 pm.up_rows};
+      up_sep_kernel<<<dim3(P.lv[l].B, 6, pm.up_nband), 256, 0, s>>>(a);
+    } else {
+      UpArg a{Sc, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
               pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
       dim3 gu(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6);
       up_kernel<<<gu, kThreads, 0, s>>>(a);
     }
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[2 + 4 * m], s));
-    // translations of every level (independent of each other) ...
+  }
+}
+
+// Translations of every level of medium m (independent of each other).
+void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
+  const int L = P.maxL;
+  if (P.tuning.m2l_variant == 3) {
+    if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+    M2lWarpArg a{};
+    int ctas = 0;
     for (int l = 2; l <= L; ++l) {
       const MediumLevel& cm = P.ml[m][l];
-      if (P.tuning.m2l_variant == 1) {
-        M2lTileArg a{cm.S, cm.Bm, P.lv[l - 1].child_begin, P.lv[l].usrc_ptr, P.lv[l].usrc, P.lv[l].coord,
-                     cm.off2vec, cm.tfw, cm.K};
-        dim3 gd(P.lv[l - 1].B, (cm.K + kTileDirs - 1) / kTileDirs);
-        m2l_tile_kernel<<<gd, kTileDirs * kTileWarps, 0, s>>>(a);
-      } else {
-        M2lArg a{cm.S, cm.Bm, P.lv[l].far_ptr, P.lv[l].far_idx, P.lv[l].far_off, cm.off2vec, cm.tfw, cm.K};
-        dim3 gd(P.lv[l].B, (cm.K + kThreads - 1) / kThreads);
-        m2l_kernel<<<gd, kThreads, 0, s>>>(a);
-      }
+      M2lWarpSeg& g = a.seg[a.nseg++];
+      g = M2lWarpSeg{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, P.lv[l].far_ptr, P.lv[l].far_idx,
+                     P.lv[l].far_vec, P.lv[l].B, cm.K, (cm.K + 31) / 32, ctas};
+      ctas += ((P.lv[l].B + kWarpBoxes - 1) / kWarpBoxes) * g.nchunk;
     }
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[3 + 4 * m], s));
-    // ... then the downward chain: level l receives level l-1 once that is final
-    for (int l = 3; l <= L; ++l) {
+    m2l_warp_kernel<<<ctas, 32 * kWarpBoxes, 0, s>>>(a);
+    return;
+  }
+  if (P.tuning.m2l_variant == 2) {
+    if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+    M2lOctArg a{};
+    int ctas = 0;
+    for (int l = 2; l <= L; ++l) {
       const MediumLevel& cm = P.ml[m][l];
-      const MediumLevel& pm = P.ml[m][l - 1];
-      if (P.tuning.l2l_variant == 1 && pm.nph <= kL2lMaxPhi) {
-        L2lSepArg b{cm.Bm,      pm.Bm,     P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.thT_ptr,
-                    cm.thT_src, cm.thT_w,  cm.phT_ptr,     cm.phT_src,     cm.phT_w, cm.nth,
-                    cm.nph,     pm.nth,    pm.nph};
-        l2l_sep_kernel<<<dim3(P.lv[l].B, 6), 256, 0, s>>>(b);
-      } else {
-        L2lArg b{cm.Bm, pm.Bm, P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.tr_ptr, cm.tr_kp, cm.tr_w, cm.K, pm.K};
-        dim3 gl(P.lv[l].B, (cm.K + kThreads - 1) / kThreads, 6);
-        l2l_kernel<<<gl, kThreads, 0, s>>>(b);
-      }
+      M2lSeg& g = a.seg[a.nseg++];
+      g = M2lSeg{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, cm.off2vec, P.lv[l].ufar_ptr, P.lv[l].ufar,
+                 P.lv[l].upack, P.lv[l - 1].child_begin, P.lv[l].octant, cm.K, (cm.K + kM2lDirs - 1) / kM2lDirs,
+                 ctas};
+      ctas += P.lv[l - 1].B * g.nchunk;
     }
+    m2l_oct_kernel<<<ctas, kM2lThreads, 0, s>>>(a);
+    return;
+  }
+  for (int l = 2; l <= L; ++l) {
+    const MediumLevel& cm = P.ml[m][l];
+    if (P.tuning.m2l_variant == 1) {
+      M2lTileArg a{level_S(P, m, l, v), level_B(P, m, l, v), P.lv[l - 1].child_begin, P.lv[l].usrc_ptr,
+                   P.lv[l].usrc,        P.lv[l].coord,       cm.off2vec,              cm.tfw,
+                   cm.K};
+      dim3 gd(P.lv[l - 1].B, (cm.K + kTileDirs - 1) / kTileDirs);
+      m2l_tile_kernel<<<gd, kTileDirs * kTileWarps, 0, s>>>(a);
+    } else {
+      M2lArg a{level_S(P, m, l, v), level_B(P, m, l, v), P.lv[l].far_ptr, P.lv[l].far_idx, P.lv[l].far_off,
+               cm.off2vec,          cm.tfw,              cm.K};
+      dim3 gd(P.lv[l].B, (cm.K + kThreads - 1) / kThreads);
+      m2l_kernel<<<gd, kThreads, 0, s>>>(a);
+    }
+  }
+}
+
+// Anterpolation down the tree: level l receives level l-1 once that is final.
+void launch_l2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
+  const int L = P.maxL;
+  for (int l = 3; l <= L; ++l) {
+    const MediumLevel& cm = P.ml[m][l];
+    const MediumLevel& pm = P.ml[m][l - 1];
+    double2* Bc = level_B(P, m, l, v);
+    if (P.tuning.l2l_variant == 1 && 6 * pm.nph <= kL2lBand) {
+      L2lSepArg b{Bc,         pm.Bm,    P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.thT_ptr,
+                  cm.thT_src, cm.thT_w, cm.phT_ptr,     cm.phT_src,     cm.phT_w, cm.nth,
+                  cm.nph,     pm.nth,   pm.nph};
+      l2l_sep_kernel<<<P.lv[l].B, 256, 0, s>>>(b);
+    } else {
+      L2lArg b{Bc, pm.Bm, P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.tr_ptr, cm.tr_kp, cm.tr_w, cm.K, pm.K};
+      dim3 gl(P.lv[l].B, (cm.K + kThreads - 1) / kThreads, 6);
+      l2l_kernel<<<gl, kThreads, 0, s>>>(b);
+    }
+  }
+}
+
+template <class Arg>
+void fill_leaf_common(const Plan& P, Arg& a) {
+  a.leaf_rwg = P.d_leaf_rwg;
+  a.rwg_box = P.d_rwg_leafbox;
+  a.leaf_ptr = P.d_leaf_ptr;
+  a.near_sptr = P.d_near_sptr;
+  a.near_src = P.d_near_src;
+  a.near_zoff = P.d_near_zoff;
+  a.near_z = P.d_near_z;
+  a.N = P.N;
+  const cplx c1 = P.k1 * P.k1 / (16.0 * kPi * kPi);
+  const cplx c2v = P.k2 * P.k2 / (16.0 * kPi * kPi);
+  a.c1 = c2(c1.real(), c1.imag());
+  a.c2 = c2(c2v.real(), c2v.imag());
+  a.etai = c2(P.etai.real(), P.etai.imag());
+}
+
+cudaEvent_t* profiler_events(Plan& P, cudaStream_t s) {
+  if (!P.prof.on) return nullptr;
+  if (P.prof.used == P.prof.sets.size()) {
+    if (P.prof.sets.size() >= 4096) throw std::runtime_error("stage profiler: read it at least every 4096 applies");
+    std::array<cudaEvent_t, StageProfiler::kEvents> set{};
+    for (auto& e : set) MLFMA_CUDA(cudaEventCreate(&e));
+    P.prof.sets.push_back(set);
+  }
+  cudaEvent_t* ev = P.prof.sets[P.prof.used++].data();
+  MLFMA_CUDA(cudaEventRecord(ev[0], s));
+  return ev;
+}
+
+}  // namespace
+
+void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
+  const int L = P.maxL;
+  cudaEvent_t* ev = profiler_events(P, s);
+  if (P.tuning.agg_variant == 1) {  // both media in one launch, timed as medium 1's aggregation
+    AggBoxArg a{};
+    for (int m = 0; m < 2; ++m) {
+      a.Vs[m] = P.d_Vs[m];
+      a.S[m] = P.ml[m][L].S;
+      a.K[m] = P.ml[m][L].K;
+    }
+    a.leaf_ptr = P.d_leaf_ptr;
+    a.leaf_rwg = P.d_leaf_rwg;
+    a.x = x;
+    a.N = P.N;
+    agg_box_kernel<<<dim3(P.lv[L].B, 2), kThreads, 0, s>>>(a);
+  }
+  for (int m = 0; m < 2; ++m) {
+    const MediumLevel& leaf = P.ml[m][L];
+    if (P.tuning.agg_variant == 0) {
+      dim3 g(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads);
+      agg_kernel<<<g, kThreads, 0, s>>>(P.d_Vs[m], P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, leaf.S);
+    }
+    if (ev) MLFMA_CUDA(cudaEventRecord(ev[1 + 4 * m], s));
+    const LeafView v{leaf.S, leaf.Bm};
+    launch_up(P, m, v, s);
+    if (ev) MLFMA_CUDA(cudaEventRecord(ev[2 + 4 * m], s));
+    launch_m2l(P, m, v, s);
+    if (ev) MLFMA_CUDA(cudaEventRecord(ev[3 + 4 * m], s));
+    launch_l2l(P, m, v, s);
     if (ev) MLFMA_CUDA(cudaEventRecord(ev[4 + 4 * m], s));
   }
   LeafArg a{};
@@ -454,25 +1035,71 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
     a.khat[m] = P.ml[m][L].khat;
     a.K[m] = P.ml[m][L].K;
   }
-  a.leaf_rwg = P.d_leaf_rwg;
-  a.rwg_box = P.d_rwg_leafbox;
-  a.leaf_ptr = P.d_leaf_ptr;
-  a.near_sptr = P.d_near_sptr;
-  a.near_src = P.d_near_src;
-  a.near_zoff = P.d_near_zoff;
-  a.near_z = P.d_near_z;
+  fill_leaf_common(P, a);
   a.x = x;
   a.w = w;
-  a.N = P.N;
-  const cplx c1 = P.k1 * P.k1 / (16.0 * kPi * kPi);
-  const cplx c2v = P.k2 * P.k2 / (16.0 * kPi * kPi);
-  a.c1 = c2(c1.real(), c1.imag());
-  a.c2 = c2(c2v.real(), c2v.imag());
-  a.etai = c2(P.etai.real(), P.etai.imag());
   const int warps = kThreads / 32;
   leaf_out_kernel<<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
   MLFMA_CUDA(cudaGetLastError());
   if (ev) MLFMA_CUDA(cudaEventRecord(ev[9], s));
+}
+
+void reserve_batch(Plan& P, int R) {
+  const int want = std::min(R, kBatchSlots);
+  const int L = P.maxL;
+  while (P.batch_cap < want) {
+    for (int m = 0; m < 2; ++m) {
+      const size_t cnt = static_cast<size_t>(P.lv[L].B) * 6 * P.ml[m][L].K;
+      P.bS[m].push_back(P.alloc<double2>(cnt));
+      P.bB[m].push_back(P.alloc<double2>(cnt));
+    }
+    ++P.batch_cap;
+  }
+}
+
+void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw, cudaStream_t s) {
+  const int L = P.maxL;
+  if (P.batch_cap < std::min(R, kBatchSlots)) throw std::runtime_error("batched apply: slots not reserved");
+  constexpr int kAggRB = 8, kLeafRB = 4;
+  for (int g0 = 0; g0 < R; g0 += kBatchSlots) {
+    const int rn = std::min(kBatchSlots, R - g0);
+    AggBatchArg ag{};
+    for (int m = 0; m < 2; ++m) {
+      ag.Vs[m] = P.d_Vs[m];
+      ag.K[m] = P.ml[m][L].K;
+      for (int j = 0; j < rn; ++j) ag.S[m][j] = P.bS[m][j];
+    }
+    ag.leaf_ptr = P.d_leaf_ptr;
+    ag.leaf_rwg = P.d_leaf_rwg;
+    ag.X = X + g0 * ldx;
+    ag.ldx = ldx;
+    ag.N = P.N;
+    ag.R = rn;
+    agg_batch_kernel<kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
+    for (int j = 0; j < rn; ++j)
+      for (int m = 0; m < 2; ++m) {
+        const LeafView v{P.bS[m][j], P.bB[m][j]};
+        launch_up(P, m, v, s);
+        launch_m2l(P, m, v, s);
+        launch_l2l(P, m, v, s);
+      }
+    LeafBatchArg lb{};
+    for (int m = 0; m < 2; ++m) {
+      lb.Vf[m] = P.d_Vf[m];
+      lb.khat[m] = P.ml[m][L].khat;
+      lb.K[m] = P.ml[m][L].K;
+      for (int j = 0; j < rn; ++j) lb.Bm[m][j] = P.bB[m][j];
+    }
+    fill_leaf_common(P, lb);
+    lb.X = X + g0 * ldx;
+    lb.ldx = ldx;
+    lb.W = W + g0 * ldw;
+    lb.ldw = ldw;
+    lb.R = rn;
+    const int warps = kThreads / 32;
+    leaf_out_batch_kernel<kLeafRB><<<dim3((P.N + warps - 1) / warps, (rn + kLeafRB - 1) / kLeafRB), kThreads, 0, s>>>(lb);
+    MLFMA_CUDA(cudaGetLastError());
+  }
 }
 
 }  // namespace mlfma

@@ -178,6 +178,41 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
       }
       D.usrc_ptr = P->upload(uptr);
       D.usrc = P->upload(usrc);
+      // per parent: union of the children's interaction-list sources with
+      // the octant mask of the children that translate each of them
+      std::vector<int> fptr(Pl.size() + 1, 0), fsrc, fpack;
+      std::vector<std::array<int, 3>> tagged;  // (source, octant, offset code)
+      for (int p = 0; p < Pl.size(); ++p) {
+        tagged.clear();
+        for (int c = Pl.child_begin[p]; c < Pl.child_begin[p + 1]; ++c) {
+          if ((Lv.ix[c] >> 1) != Pl.ix[p] || (Lv.iy[c] >> 1) != Pl.iy[p] || (Lv.iz[c] >> 1) != Pl.iz[p])
+            throw std::runtime_error("child box coordinates are not 2 * parent + octant");
+          const int o = (Lv.ix[c] & 1) | ((Lv.iy[c] & 1) << 1) | ((Lv.iz[c] & 1) << 2);
+          for (int e = Lv.far_ptr[c]; e < Lv.far_ptr[c + 1]; ++e) tagged.push_back({Lv.far_idx[e], o, Lv.far_off[e]});
+        }
+        std::sort(tagged.begin(), tagged.end());
+        for (size_t i = 0; i < tagged.size();) {
+          const int sb = tagged[i][0];
+          const int d0[3] = {2 * Pl.ix[p] - Lv.ix[sb], 2 * Pl.iy[p] - Lv.iy[sb], 2 * Pl.iz[p] - Lv.iz[sb]};
+          for (int ax = 0; ax < 3; ++ax)
+            if (d0[ax] < -3 || d0[ax] > 2) throw std::runtime_error("interaction source outside the parent neighbourhood");
+          const int enc0 = encode_offset(d0[0], d0[1], d0[2]);
+          int mask = 0;
+          for (; i < tagged.size() && tagged[i][0] == sb; ++i) {
+            const int o = tagged[i][1];
+            // the kernel forms the child's offset code as enc0 + octant offset
+            if (enc0 + (o & 1) * 49 + ((o >> 1) & 1) * 7 + (o >> 2) != tagged[i][2])
+              throw std::runtime_error("interaction offset code mismatch");
+            mask |= 1 << o;
+          }
+          fsrc.push_back(sb);
+          fpack.push_back(enc0 | (mask << 9));
+        }
+        fptr[p + 1] = static_cast<int>(fsrc.size());
+      }
+      D.ufar_ptr = P->upload(fptr);
+      D.ufar = P->upload(fsrc);
+      D.upack = P->upload(fpack);
     }
   }
   for (int m = 0; m < 2; ++m) {
@@ -196,6 +231,45 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
         const double hc = T.lv[l + 1].len;
         M.ph_up = P->upload(shift_table(M.grid, kc[m], hc, -1.0));  // parent - child
         M.ph_dn = P->upload(shift_table(M.grid, kc[m], hc, +1.0));  // child - parent
+        // bands of parent theta rows for the separable interpolation: at most
+        // kUpBandOut outputs and kUpBandEntries staged child-row entries a band
+        const int npp = M.nph;
+        std::vector<int> rows;
+        auto band_rows = [&](int t0, int R) {
+          rows.clear();
+          for (int t = t0; t < std::min(M.nth, t0 + R); ++t)
+            for (int i = 0; i < 3; ++i) rows.push_back(I.tidx[3 * t + i]);
+          std::sort(rows.begin(), rows.end());
+          rows.erase(std::unique(rows.begin(), rows.end()), rows.end());
+        };
+        auto worst_band = [&](int R) {
+          int worst = 0;
+          for (int t0 = 0; t0 < M.nth; t0 += R) {
+            band_rows(t0, R);
+            worst = std::max(worst, static_cast<int>(rows.size()));
+          }
+          return worst;
+        };
+        int R = std::max(1, std::min(M.nth, kUpBandOut / npp));
+        while (R > 1 && worst_band(R) * npp > kUpBandEntries) --R;
+        if (R * npp <= kUpBandOut && worst_band(R) * npp <= kUpBandEntries) {
+          M.up_rows = R;
+          M.up_nband = (M.nth + R - 1) / R;
+          std::vector<int> rptr(M.up_nband + 1, 0), rlist, tpos(3 * static_cast<size_t>(M.nth));
+          for (int bi = 0; bi < M.up_nband; ++bi) {
+            band_rows(bi * R, R);
+            for (int t = bi * R; t < std::min(M.nth, (bi + 1) * R); ++t)
+              for (int i = 0; i < 3; ++i)
+                tpos[3 * t + i] =
+                    static_cast<int>(std::lower_bound(rows.begin(), rows.end(), I.tidx[3 * t + i]) - rows.begin());
+            rlist.insert(rlist.end(), rows.begin(), rows.end());
+            rptr[bi + 1] = static_cast<int>(rlist.size());
+            M.up_band_max = std::max(M.up_band_max, static_cast<int>(rows.size()));
+          }
+          M.up_row_ptr = P->upload(rptr);
+          M.up_row = P->upload(rlist);
+          M.up_tpos = P->upload(tpos);
+        }
       }
       if (l > 2) {
         // transposed interpolation: child direction <- (parent direction, weight)
@@ -261,6 +335,11 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
           }
         M.nvec = static_cast<int>(M.vec_off.size());
         M.off2vec = P->upload(off2vec);
+        if (m == 0) {  // the offset -> row map depends on the level's lists only, not on the medium
+          std::vector<int> fv(T.lv[l].far_off.size());
+          for (size_t e = 0; e < fv.size(); ++e) fv[e] = off2vec[T.lv[l].far_off[e]];
+          P->lv[l].far_vec = P->upload(fv);
+        }
         std::vector<double> rhat;
         std::vector<int> hoff, hL;
         std::vector<double2> h2all;

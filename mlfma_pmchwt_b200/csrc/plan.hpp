@@ -20,6 +20,11 @@
 
 namespace mlfma {
 
+// Separable interpolation bands: outputs per band (4 per thread of a
+// 256-thread CTA) and the staged child-row entries a band may hold (40 KiB).
+constexpr int kUpBandOut = 1024;
+constexpr int kUpBandEntries = 2560;
+
 struct MediumLevel {
   int L = 0, nth = 0, nph = 0, K = 0;
   double2* S = nullptr;
@@ -35,6 +40,13 @@ struct MediumLevel {
   double* lp = nullptr;        // [nph][3]
   double2* ph_up = nullptr;    // [8][K]: exp(-j k khat.(c_parent - c_child)), child octant o
   double2* ph_dn = nullptr;    // [8][K]: exp(-j k khat.(c_child - c_parent))
+  // separable interpolation in bands of up_rows theta rows of this grid:
+  // band i needs the child theta rows up_row[up_row_ptr[i] .. up_row_ptr[i+1])
+  // and parent row t's tap i reads band row up_tpos[3 t + i]
+  int up_rows = 0, up_nband = 0, up_band_max = 0;
+  int* up_row_ptr = nullptr;
+  int* up_row = nullptr;
+  int* up_tpos = nullptr;
   // this level as child of level-1: for each child direction, the parent
   // directions that interpolate onto it and the Lagrange weight
   int* tr_ptr = nullptr;       // [K+1]
@@ -62,16 +74,29 @@ struct DevLevel {
   int* far_ptr = nullptr;      // [B+1]
   int* far_idx = nullptr;
   int* far_off = nullptr;
+  int* far_vec = nullptr;      // transfer-factor row of each interaction-list entry
   long long far_pairs = 0;
   int* coord = nullptr;        // [3 * B] integer box coordinates
   int* usrc_ptr = nullptr;     // per parent box (level - 1): union of its children's
   int* usrc = nullptr;         //   interaction sources at this level (ascending)
+  // Per parent box (level - 1): the union of its children's interaction-list
+  // sources, each with pack = enc(2 * parent - source) | (octant mask << 9);
+  // bit o of the mask is set when the child in octant o has the source in
+  // its interaction list. The child's offset code is enc + octant_offset(o).
+  int* ufar_ptr = nullptr;
+  int* ufar = nullptr;
+  int* upack = nullptr;
 };
 
 // Kernel choices a plan can be tuned with (mlfma_set_tuning).
 struct Tuning {
-  int m2l_variant = 1;         // 0: one thread per (box, direction); 1: sibling-group tiles
+  int m2l_variant = 2;         // 0: one thread per (box, direction); 1: sibling-group tiles;
+                               // 2: octant registers over the sibling union, all levels per launch;
+                               // 3: warp per box, 8 Morton-consecutive boxes per CTA, all levels per launch
   int l2l_variant = 1;         // 0: 2-D transposed taps per child direction; 1: separable
+  int up_variant = 1;          // 0: 9-tap gather per parent direction; 1: separable in bands
+  int agg_variant = 1;         // 0: thread per (box, direction); 1: CTA per (box, medium) streaming
+                               //    the box's contiguous pattern block
 };
 
 // Per-apply CUDA events between stage groups, recorded on the launching
@@ -132,6 +157,13 @@ struct Plan {
   // ---- vectors
   double2* d_x = nullptr;           // staging for host-pointer apply
   double2* d_w = nullptr;
+  // ---- batched apply: leaf-level S / B arrays of each right-hand-side slot
+  // (levels above the leaf are shared: the slots pass through them in turn)
+  int batch_cap = 0;
+  std::vector<double2*> bS[2], bB[2];
+  double2* d_xb = nullptr;          // staging for host-pointer batched apply
+  double2* d_wb = nullptr;
+  int xb_cap = 0;
   cudaStream_t stream = nullptr;
   StageProfiler prof;
   size_t bytes = 0;
@@ -189,6 +221,11 @@ void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& 
                      const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s);
 void launch_near(Plan& P, cudaStream_t s);
 void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s);
+// Batched apply: W[j] = A X[j] for j < R; X[j] at X + j * ldx (ldx >= 2N),
+// the same for W. Right-hand sides go through in groups of kBatchSlots.
+constexpr int kBatchSlots = 16;
+void reserve_batch(Plan& P, int R);  // allocates the leaf-level arrays of min(R, kBatchSlots) slots
+void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw, cudaStream_t s);
 int read_stage_times(Plan& P, double out[kStages]);
 
 }  // namespace mlfma

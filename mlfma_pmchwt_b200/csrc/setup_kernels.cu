@@ -190,7 +190,15 @@ struct SingGeom {
   double Iv1[3], Is1, Iv3[3], Is3;
 };
 
-__host__ __device__ void sing_geometry(const Tri& S, const double* r, SingGeom& o) {
+// in_plane: r is a point of S itself (the same-triangle term), so its height
+// above the source plane is exactly zero. The reference computes that height
+// as n.(r - v_i), whose roundoff (~1e-15 for coordinates of order 1) can
+// exceed its 10 eps0 threshold; it then takes the 1/|D| branch of the 1/R^3
+// integral, whose ~1e15-sized result should cancel in the K term (exactly
+// zero for a flat triangle) but leaves a residue set by the last bits of
+// atan. Using D = 0 there evaluates the reference's formulas at the exact
+// height: the same result wherever the reference stays below its threshold.
+__host__ __device__ void sing_geometry(const Tri& S, const double* r, SingGeom& o, bool in_plane) {
   const double* nS = S.n;
   double rho_v[3][3];
   for (int i = 0; i < 3; ++i) {
@@ -226,7 +234,7 @@ __host__ __device__ void sing_geometry(const Tri& S, const double* r, SingGeom& 
       for (int a = 0; a < 3; ++a) Pv[i][a] = (de[a] - ll[i][a] * Lpl[i]) / Pnul[i];
     }
     const double dv[3] = {r[0] - S.v[i][0], r[1] - S.v[i][1], r[2] - S.v[i][2]};
-    D[i] = dot3(nS, dv);
+    D[i] = in_plane ? 0.0 : dot3(nS, dv);
   }
   for (int a = 0; a < 3; ++a) {
     o.Iv1[a] = 0.0;
@@ -343,7 +351,7 @@ __host__ __device__ void rwg_pair_ops(const GeomArg& g, const QuadArg& q, int fl
           qpoint(q, p, F.v[0], F.v[1], F.v[2], rF);
           const double wF = q.w[p];
           SingGeom sg;
-          sing_geometry(S, rF, sg);
+          sing_geometry(S, rF, sg, true);
           const double RWGf[3] = {(rF[0] - vF[0]) * recAf, (rF[1] - vF[1]) * recAf, (rF[2] - vF[2]) * recAf};
           const double pv1[3] = {sg.rho[0] - rho0N[0], sg.rho[1] - rho0N[1], sg.rho[2] - rho0N[2]};
           // singL (Code/Operator.h:301-321)

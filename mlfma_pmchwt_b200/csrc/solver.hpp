@@ -25,6 +25,14 @@ bool gmres_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, dou
 bool fgmres_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, double tol_abs, double tol_rel,
                   int inner_its, SolveStats& st, std::vector<double>& history);
 
+// Lockstep FGMRES of R systems (fgmres_batch.cu): x, rhs host complex128
+// [R][2N]; per system the iteration of fgmres_solve, with every operator
+// apply and near-field product batched over the systems still iterating.
+// Returns the converged flag of each system.
+std::vector<char> fgmres_batch_solve(Plan& P, int R, double* x, const double* rhs, int itr_max, int mr,
+                                     double tol_abs, double tol_rel, int inner_its, std::vector<SolveStats>& st,
+                                     std::vector<std::vector<double>>& hist, double& seconds);
+
 // w = Z_near x on device vectors (complex128 [2N]).
 void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s);
 

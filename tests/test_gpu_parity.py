@@ -55,33 +55,41 @@ def test_transfer_factors(case_files, ref_ops, name):
 
 
 def _dense_near(op, ref):
+    """Near-field entries of both, aligned in the reference's row order:
+    (pairs, 4) arrays of (z11, z12, z21, z22) and the (target, source) pairs."""
     nr = op.near()
     ptr, ids, vals = ref.znear()
     N = op.N
     mine = {}
     for t, s, a, b, c in zip(nr["target"], nr["source"], nr["z11"], nr["z12"], nr["z22"]):
         mine[(int(t), int(s))] = (a, b, -b, c)
-    got, want = [], []
+    got, want, pairs = [], [], []
     for t in range(N):
         r1 = slice(ptr[t], ptr[t + 1])
         r2 = slice(ptr[N + t], ptr[N + t + 1])
         ids1, v1, v2 = ids[r1], vals[r1], vals[r2]
         for j in range(0, len(ids1), 2):
             s = int(ids1[j])
-            got.extend(mine[(t, s)])
-            want.extend((v1[j], v1[j + 1], v2[j], v2[j + 1]))
-    return np.array(got), np.array(want), len(mine)
+            got.append(mine[(t, s)])
+            want.append((v1[j], v1[j + 1], v2[j], v2[j + 1]))
+            pairs.append((t, s))
+    assert len(mine) == len(pairs)
+    return np.array(got), np.array(want), np.array(pairs)
 
 
-@pytest.mark.parametrize("name", ["sphere_s2", "sphere_s3_lossy"])
+# bodies on which the reference's singular K evaluation stays well-conditioned
+NEAR_CASES = ["sphere_s2", "sphere_s3_lossy", "sphere_s4_deep"]
+
+
+@pytest.mark.parametrize("name", NEAR_CASES)
 def test_near_field_entries(case_files, ref_ops, name):
     op, ref = gpu_op(case_files, name), ref_ops(name)
     got, want, pairs = _dense_near(op, ref)
-    assert pairs == op.info.near_pairs and len(want) == 4 * pairs
+    assert len(pairs) == op.info.near_pairs
     assert rel(got, want) < TABLE_TOL
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", [c for c in CASES if c != "ellipsoid_s4_deep"])
 def test_matvec_matches_reference(case_files, ref_ops, name):
     from mlfma_pmchwt_b200 import mesh as M
     op, ref = gpu_op(case_files, name), ref_ops(name)
@@ -94,6 +102,45 @@ def test_matvec_matches_reference(case_files, ref_ops, name):
     assert rel(op.apply_ax(y), ref.apply(y)) < MATVEC_TOL
     ones = np.ones(op.n, dtype=complex)
     assert rel(op.apply_ax(ones), ref.apply(ones)) < MATVEC_TOL
+
+
+def test_same_triangle_k_terms_where_the_reference_is_ill_conditioned(case_files, ref_ops):
+    """On the deep ellipsoid (coordinates up to 2 m) the reference's height of
+    a quadrature point above its own triangle, n.(r - v_i), is rounding noise
+    that at a few points exceeds its 10 eps0 threshold, so the same-triangle
+    1/R^3 integral takes the 1/|D| branch (Code/Operator.h:637-652). The
+    resulting ~1e15-sized term should cancel (the same-triangle K integral of
+    a flat triangle is zero) but leaves a residue set by the last bits of atan.
+    The product evaluates those terms at the exact height 0. Checked here:
+    every other entry matches to table tolerance, the differing entries are
+    z12 = -z21 of RWG pairs that share a triangle (a small set), and the
+    matvec matches the reference's once those entries are exchanged."""
+    from mlfma_pmchwt_b200 import mesh as M
+    name = "ellipsoid_s4_deep"
+    op, ref = gpu_op(case_files, name), ref_ops(name)
+    got, want, pairs = _dense_near(op, ref)
+    scale = np.abs(want).max()
+    off = np.abs(got - want) > TABLE_TOL * scale
+    rows = np.nonzero(off.any(axis=1))[0]
+    assert not off[:, 0].any() and not off[:, 3].any()          # L-type entries all match
+    assert np.array_equal(off[:, 1], off[:, 2])                   # z21 = -z12 on both sides
+    assert 0 < len(rows) < 1e-3 * len(pairs)
+    r = op.rwgs()
+    tri = lambda q: {int(r["face_pos"][q]), int(r["face_neg"][q])}
+    assert all(tri(t) & tri(s) for t, s in pairs[rows])
+    clean = np.ones(len(pairs), bool)
+    clean[rows] = False
+    assert rel(got[clean], want[clean]) < TABLE_TOL
+    # matvec: the reference's, with the flagged entries replaced by the product's
+    x = M.unit_disk_vector(op.n, 0)
+    wr = ref.apply(x)
+    N = op.N
+    for i in rows:
+        t, s = pairs[i]
+        d12 = got[i, 1] - want[i, 1]
+        wr[t] += d12 * x[N + s]
+        wr[N + t] += (got[i, 2] - want[i, 2]) * x[s]
+    assert rel(op.apply_ax(x), wr) < MATVEC_TOL
 
 
 @pytest.mark.parametrize("name", ["sphere_s3", "sphere_s4_deep"])
@@ -204,20 +251,25 @@ def test_error_paths_on_device_plan(case_files):
     assert e.value.code == -1
 
 
-@pytest.mark.parametrize("name", ["sphere_s3", "ellipsoid_s3"])
-def test_translation_variants_agree(case_files, ref_ops, name):
-    """Both translation kernels (per-box and sibling-group tiles) give the
-    reference's matvec, and agree with each other to rounding."""
+@pytest.mark.parametrize("name", ["sphere_s3", "ellipsoid_s3", "sphere_s4_deep"])
+def test_kernel_variants_agree(case_files, ref_ops, name):
+    """Every translation, interpolation and anterpolation kernel variant gives
+    the reference's matvec, and all agree with each other to rounding."""
     from mlfma_pmchwt_b200 import mesh as M
     op, ref = gpu_op(case_files, name), ref_ops(name)
     x = M.unit_disk_vector(op.n, 6)
     wr = ref.apply(x)
-    out = {}
-    for v in (0, 1):
-        op.set_tuning("m2l.variant", v)
-        out[v] = op.apply_ax(x)
-        assert rel(out[v], wr) < MATVEC_TOL
-    assert rel(out[1], out[0]) < 1e-13
+    base = None
+    for key, cnt in op.TUNING_KEYS:
+        keep = op.get_tuning(key)
+        for v in range(cnt):
+            op.set_tuning(key, v)
+            w = op.apply_ax(x)
+            assert rel(w, wr) < MATVEC_TOL, (key, v)
+            base = w if base is None else base
+            assert rel(w, base) < 1e-13, (key, v)
+        op.set_tuning(key, keep)
     res = op.autotune(2)
-    assert res["m2l.variant"] in (0, 1) and all(t > 0 for t in res["variant_ms"])
+    for key, cnt in op.TUNING_KEYS:
+        assert 0 <= res[key] < cnt and len(res[key + "_ms"]) == cnt and min(res[key + "_ms"]) > 0
     assert rel(op.apply_ax(x), wr) < MATVEC_TOL
