@@ -248,7 +248,7 @@ struct TuningKey {
 };
 constexpr TuningKey kTuningKeys[] = {
     {"m2l.variant", &mlfma::Tuning::m2l_variant, 4},
-    {"up.variant", &mlfma::Tuning::up_variant, 2},
+    {"up.variant", &mlfma::Tuning::up_variant, 3},
     {"l2l.variant", &mlfma::Tuning::l2l_variant, 2},
     {"agg.variant", &mlfma::Tuning::agg_variant, 2},
 };

@@ -1,4 +1,5 @@
-// complex128 helpers on double2 (x = real, y = imaginary).
+// complex128 helpers on double2 (x = real, y = imaginary), and the complex64
+// subset the mixed-precision operator uses on float2.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -47,5 +48,40 @@ __host__ __device__ __forceinline__ double2 cexp(double2 z) {
 __host__ __device__ __forceinline__ double2 cexp_mjkt(double2 k, double t) {
   return cexp(make_double2(k.y * t, -k.x * t));
 }
+
+// complex64 counterparts on float2, for the mixed-precision operator
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
+  return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
+}
+__host__ __device__ __forceinline__ float2 cfmas(float s, float2 a, float2 c) {
+  return make_float2(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y));
+}
+
+// Storage-type traits of the apply kernels: the complex type C (double2 or
+// float2), its real type, zero and conversions from / to complex128.
+template <class C>
+struct Cx;
+template <>
+struct Cx<double2> {
+  using real = double;
+  __host__ __device__ static __forceinline__ double2 zero() { return make_double2(0.0, 0.0); }
+  __host__ __device__ static __forceinline__ double2 from(double2 v) { return v; }
+  __host__ __device__ static __forceinline__ double2 to64(double2 v) { return v; }
+};
+template <>
+struct Cx<float2> {
+  using real = float;
+  __host__ __device__ static __forceinline__ float2 zero() { return make_float2(0.f, 0.f); }
+  __host__ __device__ static __forceinline__ float2 from(double2 v) {
+    return make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+  }
+  __host__ __device__ static __forceinline__ double2 to64(float2 v) { return make_double2(v.x, v.y); }
+};
 
 }  // namespace mlfma

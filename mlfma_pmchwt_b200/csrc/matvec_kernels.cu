@@ -162,6 +162,47 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg a) {
   a.Sp[(static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
 }
 
+// Interpolation (m2m), one thread per (parent box, parent direction) for all
+// 6 components: the stencil (3 theta x 3 phi taps and weights) and the
+// child's shift phase are loaded once per child and applied to the 6
+// component rows, 54 independent loads per child in flight.
+__global__ void __launch_bounds__(kThreads) up6_kernel(UpArg a) {
+  const int kk = blockIdx.y * blockDim.x + threadIdx.x;
+  const int b = blockIdx.x;
+  if (kk >= a.Kp) return;
+  const int t = kk / a.nphp, p = kk - t * a.nphp;
+  int ti[3], pi[3];
+  double wt[3], wp[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    ti[i] = __ldg(a.tidx + 3 * t + i) * a.nphc;
+    wt[i] = __ldg(a.lt + 3 * t + i);
+    pi[i] = __ldg(a.pidx + 3 * p + i);
+    wp[i] = __ldg(a.lp + 3 * p + i);
+  }
+  double2 acc[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) acc[c] = c2(0.0, 0.0);
+  const int c1 = a.child_begin[b + 1];
+  for (int ch = a.child_begin[b]; ch < c1; ++ch) {
+    const double2 e = __ldg(a.ph_up + a.octant[ch] * a.Kp + kk);
+    const double2* sc = a.Sc + static_cast<size_t>(ch) * 6 * a.Kc;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      const double2* sr = sc + static_cast<size_t>(c) * a.Kc;
+      double2 v = c2(0.0, 0.0);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) v = cfmas(wt[i] * wp[j], __ldg(sr + ti[i] + pi[j]), v);
+      acc[c] = cfma(e, v, acc[c]);
+    }
+  }
+  double2* out = a.Sp + static_cast<size_t>(b) * 6 * a.Kp + kk;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * a.Kp] = acc[c];
+}
+
 struct UpSepArg {
   const double2* Sc;   // child level patterns [Bc][6][Kc]
   double2* Sp;         // parent level patterns [Bp][6][Kp]
@@ -881,7 +922,11 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
     const MediumLevel& pm = P.ml[m][l];
     const MediumLevel& cm = P.ml[m][l + 1];
     const double2* Sc = level_S(P, m, l + 1, v);
-    if (P.tuning.up_variant == 1 && pm.up_rows > 0) {
+    if (P.tuning.up_variant == 2) {
+      UpArg a{Sc, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
+              pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
+      up6_kernel<<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads), kThreads, 0, s>>>(a);
+    } else if (P.tuning.up_variant == 1 && pm.up_rows > 0) {
       UpSepArg a{Sc,    pm.S,     P.lv[l].child_begin, P.lv[l + 1].octant, pm.pidx,
                  pm.lp, pm.lt,    pm.up_row_ptr,       pm.up_row,          pm.up_tpos,
                  pm.ph_up, pm.nth, pm.nph,             cm.nph,             cm.K,

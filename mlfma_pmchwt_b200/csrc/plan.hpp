@@ -94,7 +94,8 @@ struct Tuning {
                                // 2: octant registers over the sibling union, all levels per launch;
                                // 3: warp per box, 8 Morton-consecutive boxes per CTA, all levels per launch
   int l2l_variant = 1;         // 0: 2-D transposed taps per child direction; 1: separable
-  int up_variant = 1;          // 0: 9-tap gather per parent direction; 1: separable in bands
+  int up_variant = 1;          // 0: 9-tap gather per parent direction; 1: separable in bands;
+                               // 2: 9-tap gather, all 6 components per thread
   int agg_variant = 1;         // 0: thread per (box, direction); 1: CTA per (box, medium) streaming
                                //    the box's contiguous pattern block
 };
