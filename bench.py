@@ -253,7 +253,8 @@ def run_product(args):
     wl = workload(args)
     m = M.icosphere(wl["sub"], wl["radius"])
     t0 = time.perf_counter()
-    op = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local)
+    op = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local,
+               precision="mixed" if args.mixed else "fp64")
     setup_s = time.perf_counter() - t0
     n = op.n
     x_host = M.unit_disk_vector(n, 0)
@@ -333,6 +334,25 @@ def run_product(args):
                 "matvec_bytes": sum(sb.values()),
                 "matvec_frac": round(sum(sb.values()) / (ms_per_step / 1000.0) / 1e9 / peak, 4)}
 
+    # the complex64 operator of the same plan (mixed precision), same timing
+    mixed = None
+    if args.mixed:
+        wm = torch.empty_like(w)
+        for _ in range(3):
+            op.apply_mixed_device(x.data_ptr(), wm.data_ptr(), sp)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            op.apply_mixed_device(x.data_ptr(), wm.data_ptr(), sp)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        mms = allreduce_max(e0.elapsed_time(e1), world, dev) / args.steps
+        step()
+        torch.cuda.synchronize(dev)
+        err = float(torch.linalg.vector_norm(wm - w) / torch.linalg.vector_norm(w))
+        mixed = {"value": round(world * 1000.0 / mms, 3), "unit": UNIT, "ms_per_step": round(mms, 4),
+                 "dtype": "c64 tables and arithmetic, c128 vectors", "rel_diff_vs_fp64_apply": err}
+
     # Solves of the plane-wave excitation (x-polarised, incident along -z) to
     # 1e-3 relative residual. (1) The reference's operator (real-argument
     # transfer factors, as Code/AlgoMLFMM.h:259-281 evaluates them for the
@@ -352,13 +372,21 @@ def run_product(args):
         if wl["eps"].imag != 0.0:
             op.close()
             opc = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local,
-                        tf_complex_argument=True)
+                        tf_complex_argument=True, precision="mixed" if args.mixed else "fp64")
             for k, v in tune.items():
                 if not k.endswith("_ms"):
                     opc.set_tuning(k, v)
             _, sc = opc.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
                                       inner_its=args.inner_its)
             solve["complex_transfer"] = solve_record(sc, args.inner_its)
+            if args.mixed:
+                _, sm = opc.solve_mixed(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
+                                        inner_its=args.inner_its, refine_max=10)
+                rec = solve_record(sm, args.inner_its)
+                rec["solver"] = ("FP64 iterative refinement around complex64 " + rec["solver"] +
+                                 "; residual checked with the FP64 operator")
+                rec["refinements"] = sm["refinements"]
+                solve["complex_transfer_mixed"] = rec
             op = opc
 
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -371,6 +399,8 @@ def run_product(args):
             "e2e": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in e2e.items()},
             "gpu_launches": args.steps * launches_per_apply(op.max_level, tune),
             "roofline": roofline, "clocks": clk}
+    if mixed:
+        line["mixed_precision"] = mixed
     if solve:
         line["solve"] = solve
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -403,6 +433,8 @@ def main(argv=None):
     ap.add_argument("--plain-its", type=int, default=300, help="iteration cap of the plain GMRES comparison")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference matvecs to time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", dest="mixed", action="store_false",
+                    help="skip the complex64 (mixed-precision) operator and solve")
     ap.add_argument("--tuning", default="auto",
                     help="'auto' (autotune) or fixed kernel variants, e.g. m2l.variant=2,up.variant=1")
     args = ap.parse_args(argv)

@@ -61,7 +61,9 @@ typedef struct {
   double mu_r_re, mu_r_im;
   double leaf_coeff;           /* leaf box edge in wavelengths (Code/PhyConstant.h:14; 0.3) */
   int gauss_points;            /* triangle rule: 1,3,4,6,7,12,13,16 (Code/GaussPoints.cpp:286-299) */
-  int precision;               /* MLFMA_PREC_FP64 */
+  int precision;               /* MLFMA_PREC_FP64, or MLFMA_PREC_MIXED: the plan also holds
+                                  complex64 copies of its tables for mlfma_apply_mixed_device
+                                  and the mixed-precision solves */
   int device;                  /* CUDA device ordinal */
   int verbose;                 /* print setup summary to stderr */
   int tf_complex_argument;     /* 0 (default): transfer factors with h2_l(|kR|) as the reference
@@ -70,6 +72,7 @@ typedef struct {
 } mlfma_params;
 
 #define MLFMA_PREC_FP64 0
+#define MLFMA_PREC_MIXED 1
 
 typedef struct {
   int num_rwg;                 /* N */
@@ -210,6 +213,33 @@ MLFMA_API int mlfma_fgmres(mlfma_plan* plan, int n, double* x, const double* rhs
  * converged, MLFMA_ERR_NOT_CONVERGED otherwise. */
 MLFMA_API int mlfma_fgmres_batch(mlfma_plan* plan, int n, int R, double* x, const double* rhs, int itr_max, int mr,
                                  double tol_abs, double tol_rel, int inner_its, mlfma_solve_stats* stats);
+
+/* Mixed precision (plans created with precision = MLFMA_PREC_MIXED; no
+ * counterpart in the reference, which is FP64 throughout). The complex64
+ * operator keeps complex128 x and w but holds the radiation/receive
+ * patterns, transfer factors, shift phases, near field and Sm/Bm workspaces
+ * in complex64 and computes in FP32; its relative difference from the FP64
+ * operator is about 1e-6. */
+MLFMA_API int mlfma_apply_mixed(mlfma_plan* plan, int n, const double* x, double* w);
+MLFMA_API int mlfma_apply_mixed_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream);
+
+/* FP64 iterative refinement: up to refine_max steps of
+ *   r = b - A x (FP64 operator, the plain path); stop when ||r||/||b|| < tol_rel
+ *   (or < tol_abs); d = FGMRES(mr) on A d = r with the complex64 operator and
+ *   inner_its complex64 near-field steps as preconditioner, to the relative
+ *   tolerance max(1e-5, min(0.5, tol_rel / (2 ||r||/||b||))); x += d.
+ * The stopping test is always the FP64 residual. itr_max bounds the FGMRES
+ * iterations summed over the steps; stats->restarts = refinement steps;
+ * history[i] = FP64 relative residual after step i (entry 0: initial). */
+MLFMA_API int mlfma_solve_mixed(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr,
+                                double tol_abs, double tol_rel, int inner_its, int refine_max,
+                                mlfma_solve_stats* stats, double* history, int history_cap);
+/* The same for R right-hand sides (x, rhs: R vectors one after the other):
+ * FP64 residuals by batched applies, corrections by lockstep FGMRES with the
+ * complex64 operator (mlfma_fgmres_batch's iteration). stats: R entries. */
+MLFMA_API int mlfma_solve_mixed_batch(mlfma_plan* plan, int n, int R, double* x, const double* rhs, int itr_max,
+                                      int mr, double tol_abs, double tol_rel, int inner_its, int refine_max,
+                                      mlfma_solve_stats* stats);
 
 /* w = Z_near x on device vectors: the near-field rows alone (the product of
  * Code/MLFMM.cpp:353-366 without the far field). Asynchronous on stream. */

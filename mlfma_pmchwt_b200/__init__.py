@@ -91,6 +91,12 @@ SIGNATURES = {
                                C.POINTER(SolveStats), _DP, C.c_int]),
     "mlfma_fgmres_batch": (C.c_int, [_P, C.c_int, C.c_int, _DP, _DP, C.c_int, C.c_int, C.c_double, C.c_double,
                                      C.c_int, C.POINTER(SolveStats)]),
+    "mlfma_apply_mixed": (C.c_int, [_P, C.c_int, _DP, _DP]),
+    "mlfma_apply_mixed_device": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "mlfma_solve_mixed": (C.c_int, [_P, C.c_int, _DP, _DP, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                    C.c_int, C.POINTER(SolveStats), _DP, C.c_int]),
+    "mlfma_solve_mixed_batch": (C.c_int, [_P, C.c_int, C.c_int, _DP, _DP, C.c_int, C.c_int, C.c_double, C.c_double,
+                                          C.c_int, C.c_int, C.POINTER(SolveStats)]),
     "mlfma_apply_near_device": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "mlfma_rhs_pmchwt": (C.c_int, [_P, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt": (C.c_int, [_P, _DP, C.c_int, _DP, _DP, _DP, _DP]),
@@ -181,7 +187,8 @@ class MLFMM:
 
     def __init__(self, mesh: Mesh | None = None, *, nas_path: str | None = None, freq: float = 3.0e8,
                  eps_r: complex = 4.0, mu_r: complex = 1.0, leaf_coeff: float = 0.3, gauss_points: int = 7,
-                 device: int = 0, verbose: bool = False, tf_complex_argument: bool = False):
+                 device: int = 0, verbose: bool = False, tf_complex_argument: bool = False,
+                 precision: str = "fp64"):
         self._lib = load_library()
         prm = Params()
         self._lib.mlfma_default_params(C.byref(prm))
@@ -190,6 +197,9 @@ class MLFMM:
         prm.mu_r_re, prm.mu_r_im = mu_r.real, mu_r.imag
         prm.leaf_coeff, prm.gauss_points, prm.device, prm.verbose = leaf_coeff, gauss_points, device, int(verbose)
         prm.tf_complex_argument = int(tf_complex_argument)
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        prm.precision = 1 if precision == "mixed" else 0
         self.params = prm
         h = _P()
         if nas_path is not None:
@@ -362,6 +372,55 @@ class MLFMM:
         stats = [dict(iterations=s.iterations, restarts=s.restarts, matvecs=s.matvecs, converged=bool(s.converged),
                       rel_residual=s.rel_residual, seconds=s.seconds, near_products=s.near_products) for s in st]
         return X, stats
+
+    def apply_ax_mixed(self, x) -> np.ndarray:
+        """w = A x with the complex64 operator (plans created with precision='mixed')."""
+        x = _c128(x)
+        if x.shape != (self.n,):
+            raise ValueError(f"x must have shape ({self.n},)")
+        w = np.empty(self.n, dtype=np.complex128)
+        self._check(self._lib.mlfma_apply_mixed(self._h, self.n, _dp(x.view(np.float64)), _dp(w.view(np.float64))))
+        return w
+
+    def apply_mixed_device(self, x_ptr: int, w_ptr: int, stream: int | None = None):
+        self._check(self._lib.mlfma_apply_mixed_device(self._h, self.n, C.c_void_p(x_ptr), C.c_void_p(w_ptr),
+                                                       C.c_void_p(stream or 0)))
+
+    def solve_mixed(self, rhs, x0=None, itr_max: int | None = None, mr: int = 50, tol_abs: float = 1e-8,
+                    tol_rel: float = 1e-4, inner_its: int = 16, refine_max: int = 10):
+        """FP64 iterative refinement around complex64 FGMRES (mlfma_solve_mixed).
+        Returns (x, stats); stats["history"] holds the FP64 relative residual
+        after each refinement step (entry 0: initial)."""
+        b = _c128(rhs)
+        x = np.zeros(self.n, dtype=np.complex128) if x0 is None else _c128(x0).copy()
+        itr_max = self.n if itr_max is None else int(itr_max)
+        st = SolveStats()
+        hist = np.zeros(refine_max + 1, dtype=np.float64)
+        rc = self._lib.mlfma_solve_mixed(self._h, self.n, _dp(x.view(np.float64)), _dp(b.view(np.float64)), itr_max,
+                                         mr, tol_abs, tol_rel, int(inner_its), int(refine_max), C.byref(st),
+                                         _dp(hist), len(hist))
+        self._check(rc)
+        return x, dict(iterations=st.iterations, refinements=st.restarts, matvecs=st.matvecs,
+                       converged=bool(st.converged), rel_residual=st.rel_residual, seconds=st.seconds,
+                       near_products=st.near_products, history=hist[: st.history_len].copy())
+
+    def solve_mixed_batch(self, rhs, x0=None, itr_max: int | None = None, mr: int = 50, tol_abs: float = 1e-8,
+                          tol_rel: float = 1e-4, inner_its: int = 16, refine_max: int = 10):
+        """solve_mixed for the rows of rhs (complex128 [R, 2N]) in lockstep
+        (mlfma_solve_mixed_batch). Returns (X, list of per-system stats)."""
+        B = np.ascontiguousarray(rhs, dtype=np.complex128)
+        if B.ndim != 2 or B.shape[1] != self.n:
+            raise ValueError(f"rhs must have shape (R, {self.n})")
+        R = B.shape[0]
+        X = np.zeros_like(B) if x0 is None else np.ascontiguousarray(x0, dtype=np.complex128).copy()
+        itr_max = self.n if itr_max is None else int(itr_max)
+        st = (SolveStats * R)()
+        rc = self._lib.mlfma_solve_mixed_batch(self._h, self.n, R, _dp(X.view(np.float64)), _dp(B.view(np.float64)),
+                                               itr_max, mr, tol_abs, tol_rel, int(inner_its), int(refine_max), st)
+        self._check(rc)
+        return X, [dict(iterations=s.iterations, refinements=s.restarts, matvecs=s.matvecs,
+                        converged=bool(s.converged), rel_residual=s.rel_residual, seconds=s.seconds,
+                        near_products=s.near_products) for s in st]
 
     def apply_near_device(self, x_ptr: int, w_ptr: int, stream: int | None = None):
         """w = Z_near x on device pointers (the near-field rows alone)."""

@@ -55,6 +55,7 @@ mlfma::PlanParams to_params(const mlfma_params* p) {
   q.device = p->device;
   q.verbose = p->verbose;
   q.tf_complex_argument = p->tf_complex_argument;
+  q.precision = p->precision == MLFMA_PREC_MIXED ? 1 : 0;
   return q;
 }
 
@@ -78,13 +79,14 @@ void mlfma_default_params(mlfma_params* p) {
 
 const char* mlfma_last_error(void) { return g_last_error.c_str(); }
 
-const char* mlfma_version(void) { return "mlfma_pmchwt_b200 0.1 (sm_100a, FP64)"; }
+const char* mlfma_version(void) { return "mlfma_pmchwt_b200 0.2 (sm_100a, FP64 and mixed complex64/FP64)"; }
 
 int mlfma_plan_create(const mlfma_mesh* mesh, const mlfma_params* params, mlfma_plan** plan) {
   if (!mesh || !params || !plan) return fail(MLFMA_ERR_ARG, "null argument");
   *plan = nullptr;
   return guarded([&] {
-    if (params->precision != MLFMA_PREC_FP64) return fail(MLFMA_ERR_UNSUPPORTED, "precision");
+    if (params->precision != MLFMA_PREC_FP64 && params->precision != MLFMA_PREC_MIXED)
+      return fail(MLFMA_ERR_ARG, "precision must be MLFMA_PREC_FP64 or MLFMA_PREC_MIXED");
     mlfma::Mesh m;
     std::string err;
     if (!mlfma::mesh_from_arrays(mesh->num_points, mesh->point_ids, mesh->xyz, mesh->num_faces, mesh->face_ids,
@@ -100,7 +102,8 @@ int mlfma_plan_create_nas(const char* nas_path, const mlfma_params* params, mlfm
   if (!nas_path || !params || !plan) return fail(MLFMA_ERR_ARG, "null argument");
   *plan = nullptr;
   return guarded([&] {
-    if (params->precision != MLFMA_PREC_FP64) return fail(MLFMA_ERR_UNSUPPORTED, "precision");
+    if (params->precision != MLFMA_PREC_FP64 && params->precision != MLFMA_PREC_MIXED)
+      return fail(MLFMA_ERR_ARG, "precision must be MLFMA_PREC_FP64 or MLFMA_PREC_MIXED");
     mlfma::Mesh m;
     std::string err;
     if (!mlfma::read_nas(nas_path, m, err)) return fail(MLFMA_ERR_MESH, err);
@@ -402,6 +405,92 @@ int mlfma_fgmres_batch(mlfma_plan* plan, int n, int R, double* x, const double* 
         stats[q].history_len = 0;
         stats[q].near_products = st[q].near_products;
       }
+    }
+    return all ? MLFMA_OK : MLFMA_ERR_NOT_CONVERGED;
+  });
+}
+
+namespace {
+bool mixed_plan(const mlfma_plan* plan) { return device_plan(plan) && plan->p->precision == 1; }
+void fill_stats(mlfma_solve_stats* out, const mlfma::SolveStats& st, bool ok, int history_len) {
+  out->iterations = st.iterations;
+  out->restarts = st.restarts;
+  out->matvecs = st.matvecs;
+  out->converged = ok ? 1 : 0;
+  out->rel_residual = st.rel_residual;
+  out->seconds = st.seconds;
+  out->history_len = history_len;
+  out->near_products = st.near_products;
+}
+}  // namespace
+
+int mlfma_apply_mixed(mlfma_plan* plan, int n, const double* x, double* w) {
+  if (!plan || !plan->p || !x || !w) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (!mixed_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan was not created with MLFMA_PREC_MIXED on a device");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    const size_t bytes = static_cast<size_t>(n) * sizeof(double2);
+    MLFMA_CUDA(cudaMemcpyAsync(P.d_x, x, bytes, cudaMemcpyHostToDevice, P.stream));
+    mlfma::apply_mixed_device(P, P.d_x, P.d_w, P.stream);
+    MLFMA_CUDA(cudaMemcpyAsync(w, P.d_w, bytes, cudaMemcpyDeviceToHost, P.stream));
+    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_apply_mixed_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream) {
+  if (!plan || !plan->p || !x_dev || !w_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (x_dev == w_dev) return fail(MLFMA_ERR_ARG, "x and w must not alias");
+  if (!mixed_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan was not created with MLFMA_PREC_MIXED on a device");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::apply_mixed_device(P, static_cast<const double2*>(x_dev), static_cast<double2*>(w_dev), s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_solve_mixed(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr, double tol_abs,
+                      double tol_rel, int inner_its, int refine_max, mlfma_solve_stats* stats, double* history,
+                      int history_cap) {
+  if (!plan || !plan->p || !x || !rhs) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (mr <= 0 || mr > 63 || itr_max < 0 || inner_its < 0 || inner_its > 63 || refine_max < 0)
+    return fail(MLFMA_ERR_ARG, "need 1 <= mr <= 63, 0 <= inner_its <= 63, itr_max >= 0, refine_max >= 0");
+  if (!mixed_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan was not created with MLFMA_PREC_MIXED on a device");
+  return guarded([&] {
+    mlfma::SolveStats st;
+    std::vector<double> hist;
+    const bool ok =
+        mlfma::mixed_solve(*plan->p, x, rhs, itr_max, mr, tol_abs, tol_rel, inner_its, refine_max, st, hist);
+    const int len = static_cast<int>(std::min<size_t>(hist.size(), history ? history_cap : 0));
+    if (stats) fill_stats(stats, st, ok, len);
+    for (int i = 0; i < len; ++i) history[i] = hist[i];
+    return ok ? MLFMA_OK : MLFMA_ERR_NOT_CONVERGED;
+  });
+}
+
+int mlfma_solve_mixed_batch(mlfma_plan* plan, int n, int R, double* x, const double* rhs, int itr_max, int mr,
+                            double tol_abs, double tol_rel, int inner_its, int refine_max, mlfma_solve_stats* stats) {
+  if (!plan || !plan->p || !x || !rhs) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (R <= 0) return fail(MLFMA_ERR_ARG, "R must be positive");
+  if (mr <= 0 || mr > 63 || itr_max < 0 || inner_its < 0 || inner_its > 63 || refine_max < 0)
+    return fail(MLFMA_ERR_ARG, "need 1 <= mr <= 63, 0 <= inner_its <= 63, itr_max >= 0, refine_max >= 0");
+  if (!mixed_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan was not created with MLFMA_PREC_MIXED on a device");
+  return guarded([&] {
+    std::vector<mlfma::SolveStats> st;
+    double seconds = 0.0;
+    const std::vector<char> ok = mlfma::mixed_batch_solve(*plan->p, R, x, rhs, itr_max, mr, tol_abs, tol_rel,
+                                                          inner_its, refine_max, st, seconds);
+    bool all = true;
+    for (int q = 0; q < R; ++q) {
+      all = all && ok[q];
+      if (stats) fill_stats(&stats[q], st[q], ok[q], 0);
     }
     return all ? MLFMA_OK : MLFMA_ERR_NOT_CONVERGED;
   });

@@ -63,6 +63,15 @@ __host__ __device__ __forceinline__ float2 cfmas(float s, float2 a, float2 c) {
   return make_float2(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y));
 }
 
+__host__ __device__ __forceinline__ float2 cdiv(float2 a, float2 b) {
+  if (fabsf(b.x) >= fabsf(b.y)) {
+    const float r = b.y / b.x, d = b.x + b.y * r;
+    return make_float2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  }
+  const float r = b.x / b.y, d = b.x * r + b.y;
+  return make_float2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+
 // Storage-type traits of the apply kernels: the complex type C (double2 or
 // float2), its real type, zero and conversions from / to complex128.
 template <class C>

@@ -22,6 +22,7 @@ namespace {
 
 using C = std::complex<double>;
 
+template <class Z>
 struct NearArg {
   const int* leaf_rwg;
   const int* rwg_box;
@@ -29,14 +30,16 @@ struct NearArg {
   const int* near_sptr;
   const int* near_src;
   const long long* near_zoff;
-  const double2* near_z;
+  const Z* near_z;
   const double2* x;
   double2* w;
   int N;
 };
 
-// w = Z_near x: rows t and N + t of the near field, one warp per RWG.
-__global__ void __launch_bounds__(128) near_apply_kernel(NearArg a) {
+// w = Z_near x: rows t and N + t of the near field, one warp per RWG; the
+// entries and the arithmetic in the storage type Z (complex128 or complex64).
+template <class Z>
+__global__ void __launch_bounds__(128) near_apply_kernel(NearArg<Z> a) {
   const int lane = threadIdx.x & 31;
   const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   if (r >= a.N) return;
@@ -44,12 +47,12 @@ __global__ void __launch_bounds__(128) near_apply_kernel(NearArg a) {
   const int b = a.rwg_box[id];
   const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
   const int tl = r - a.leaf_ptr[b];
-  const double2* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
-  double2 nJ = c2(0, 0), nM = c2(0, 0);
+  const Z* Zr = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
+  Z nJ = Cx<Z>::zero(), nM = Cx<Z>::zero();
   for (int j = lane; j < ns; j += 32) {
     const int s = a.near_src[s0 + j];
-    const double2 xJ = a.x[s], xM = a.x[a.N + s];
-    const double2 z11 = Z[3 * j], z12 = Z[3 * j + 1], z22 = Z[3 * j + 2];
+    const Z xJ = Cx<Z>::from(a.x[s]), xM = Cx<Z>::from(a.x[a.N + s]);
+    const Z z11 = Zr[3 * j], z12 = Zr[3 * j + 1], z22 = Zr[3 * j + 2];
     nJ = cfma(z11, xJ, cfma(z12, xM, nJ));
     nM = cfma(z22, xM, csub(nM, cmul(z12, xJ)));
   }
@@ -61,8 +64,8 @@ __global__ void __launch_bounds__(128) near_apply_kernel(NearArg a) {
     nM.y += __shfl_xor_sync(0xffffffffu, nM.y, o);
   }
   if (lane == 0) {
-    a.w[id] = nJ;
-    a.w[a.N + id] = nM;
+    a.w[id] = Cx<Z>::to64(nJ);
+    a.w[a.N + id] = Cx<Z>::to64(nM);
   }
 }
 
@@ -82,15 +85,29 @@ void back_substitute(const std::vector<C>& H, int ld, const std::vector<C>& s, i
 
 }  // namespace
 
-void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s) {
-  NearArg a{P.d_leaf_rwg, P.d_rwg_leafbox, P.d_leaf_ptr, P.d_near_sptr, P.d_near_src,
-            P.d_near_zoff, P.d_near_z,     x,            w,             P.N};
-  near_apply_kernel<<<(P.N + 3) / 4, 128, 0, s>>>(a);
+void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s, int prec) {
+  if (prec == 1) {
+    if (P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
+    NearArg<float2> a{P.d_leaf_rwg,  P.d_rwg_leafbox, P.d_leaf_ptr, P.d_near_sptr, P.d_near_src,
+                      P.d_near_zoff, P.d_near_z32,    x,            w,             P.N};
+    near_apply_kernel<float2><<<(P.N + 3) / 4, 128, 0, s>>>(a);
+  } else {
+    NearArg<double2> a{P.d_leaf_rwg,  P.d_rwg_leafbox, P.d_leaf_ptr, P.d_near_sptr, P.d_near_src,
+                       P.d_near_zoff, P.d_near_z,      x,            w,             P.N};
+    near_apply_kernel<double2><<<(P.N + 3) / 4, 128, 0, s>>>(a);
+  }
   MLFMA_CUDA(cudaGetLastError());
 }
 
 bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, double tol_abs, double tol_rel,
-                  int inner_its, SolveStats& st, std::vector<double>& history) {
+                  int inner_its, SolveStats& st, std::vector<double>& history, int prec) {
+  if (prec == 1 && P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
+  auto op_apply = [&](const double2* in, double2* out, cudaStream_t s) {
+    if (prec == 1)
+      apply_mixed_device(P, in, out, s);
+    else
+      apply_device(P, in, out, s);
+  };
   if (mr < 1 || mr + 1 > blas1::kMaxBasis) throw std::invalid_argument("mr must be in 1..63");
   if (inner_its < 0 || inner_its + 1 > blas1::kMaxBasis) throw std::invalid_argument("inner_its must be in 0..63");
   const auto t0 = std::chrono::steady_clock::now();
@@ -115,7 +132,7 @@ bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, d
   std::vector<C> hcol;
 
   auto true_residual = [&]() {
-    apply_device(P, x, w, s);
+    op_apply(x, w, s);
     st.matvecs++;
     return ops.residual(b, w, r);
   };
@@ -139,7 +156,7 @@ bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, d
     int used = 0;
     for (int j = 0; j < inner_its; ++j) {
       double2* u = Q + static_cast<long long>(j + 1) * n;
-      near_apply(P, Q + static_cast<long long>(j) * n, u, s);
+      near_apply(P, Q + static_cast<long long>(j) * n, u, s, prec);
       st.near_products++;
       const double hn = ops.orthogonalise(Q, j + 1, u, hcol);
       for (int i = 0; i <= j; ++i) Hi[i + j * ld] = hcol[i];
@@ -182,7 +199,7 @@ bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, d
       const double2* vk = V + static_cast<long long>(k) * n;
       double2* zk = Zd + static_cast<long long>(k) * n;
       if (inner_its > 0) precondition(vk, zk);
-      apply_device(P, zk, w, s);
+      op_apply(zk, w, s);
       st.matvecs++;
       const double h_next = ops.orthogonalise(V, k + 1, w, hcol);
       for (int j = 0; j <= k; ++j) H[j + static_cast<size_t>(k) * ld] = hcol[j];

@@ -184,6 +184,7 @@ __global__ void copy_b(VecRef src, VecRef dst, const int* sys, long long n) {
 
 // w_a = Z_near x_a for every position (warp per RWG, 4 right-hand sides per
 // warp): the near-field rows of the plan, read once per group of four.
+template <class Z>
 struct NearBatchArg {
   const int* leaf_rwg;
   const int* rwg_box;
@@ -191,7 +192,7 @@ struct NearBatchArg {
   const int* near_sptr;
   const int* near_src;
   const long long* near_zoff;
-  const double2* near_z;
+  const Z* near_z;
   VecRef x, w;
   const int* sys;
   int N, R;
@@ -199,7 +200,8 @@ struct NearBatchArg {
 
 constexpr int kNearRB = 4;
 
-__global__ void __launch_bounds__(128) near_batch_kernel(NearBatchArg a) {
+template <class Z>
+__global__ void __launch_bounds__(128) near_batch_kernel(NearBatchArg<Z> a) {
   const int lane = threadIdx.x & 31;
   const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   if (r >= a.N) return;
@@ -208,21 +210,21 @@ __global__ void __launch_bounds__(128) near_batch_kernel(NearBatchArg a) {
   const int b = a.rwg_box[id];
   const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
   const int tl = r - a.leaf_ptr[b];
-  const double2* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
-  double2 nJ[kNearRB], nM[kNearRB];
+  const Z* Zr = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
+  Z nJ[kNearRB], nM[kNearRB];
   const double2* xs[kNearRB];
 #pragma unroll
   for (int j = 0; j < kNearRB; ++j) {
-    nJ[j] = nM[j] = c2(0.0, 0.0);
+    nJ[j] = nM[j] = Cx<Z>::zero();
     xs[j] = j < pn ? a.x.at(p0 + j, a.sys) : nullptr;
   }
   for (int q = lane; q < ns; q += 32) {
     const int src = a.near_src[s0 + q];
-    const double2 z11 = Z[3 * q], z12 = Z[3 * q + 1], z22 = Z[3 * q + 2];
+    const Z z11 = Zr[3 * q], z12 = Zr[3 * q + 1], z22 = Zr[3 * q + 2];
 #pragma unroll
     for (int j = 0; j < kNearRB; ++j) {
       if (j < pn) {
-        const double2 xJ = xs[j][src], xM = xs[j][a.N + src];
+        const Z xJ = Cx<Z>::from(xs[j][src]), xM = Cx<Z>::from(xs[j][a.N + src]);
         nJ[j] = cfma(z11, xJ, cfma(z12, xM, nJ[j]));
         nM[j] = cfma(z22, xM, csub(nM[j], cmul(z12, xJ)));
       }
@@ -239,8 +241,8 @@ __global__ void __launch_bounds__(128) near_batch_kernel(NearBatchArg a) {
     }
     if (lane == 0 && j < pn) {
       double2* w = a.w.at(p0 + j, a.sys);
-      w[id] = nJ[j];
-      w[a.N + id] = nM[j];
+      w[id] = Cx<Z>::to64(nJ[j]);
+      w[a.N + id] = Cx<Z>::to64(nM[j]);
     }
   }
 }
@@ -329,8 +331,9 @@ struct BatchOps {
 
 std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* rhs, int itr_max, int mr, double tol_abs,
                         double tol_rel, int inner_its, std::vector<SolveStats>& st,
-                        std::vector<std::vector<double>>& hist, double& seconds) {
+                        std::vector<std::vector<double>>& hist, double& seconds, int prec) {
   if (R < 1) throw std::invalid_argument("R must be positive");
+  if (prec == 1 && P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
   if (mr < 1 || mr + 1 > blas1::kMaxBasis) throw std::invalid_argument("mr must be in 1..63");
   if (inner_its < 0 || inner_its + 1 > blas1::kMaxBasis) throw std::invalid_argument("inner_its must be in 0..63");
   const auto t0 = std::chrono::steady_clock::now();
@@ -385,7 +388,10 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
       std::vector<int> part(list.begin() + g0, list.begin() + g0 + rn);
       set_sys(part);
       ops.copy(rn, sysd, in, posref(Xs));
-      apply_batch_device(P, rn, Xs, n, Ws, n, s);
+      if (prec == 1)
+        apply_batch_mixed_device(P, rn, Xs, n, Ws, n, s);
+      else
+        apply_batch_device(P, rn, Xs, n, Ws, n, s);
       ops.copy(rn, sysd, posref(Ws), out);
       for (int q : part) st[q].matvecs++;
     }
@@ -415,9 +421,20 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
     std::vector<std::vector<C>> hcol;
     std::vector<double> hn;
     for (int j = 0; j < inner_its; ++j) {
-      NearBatchArg na{P.d_leaf_rwg, P.d_rwg_leafbox, P.d_leaf_ptr, P.d_near_sptr, P.d_near_src, P.d_near_zoff,
-                      P.d_near_z,   sysref(Q, qs, j * n), sysref(Q, qs, (j + 1) * n), sysd, P.N, Ra};
-      near_batch_kernel<<<dim3((P.N + 3) / 4, (Ra + kNearRB - 1) / kNearRB), 128, 0, s>>>(na);
+      const dim3 ng((P.N + 3) / 4, (Ra + kNearRB - 1) / kNearRB);
+      if (prec == 1) {
+        NearBatchArg<float2> na{P.d_leaf_rwg,  P.d_rwg_leafbox,      P.d_leaf_ptr,
+                                P.d_near_sptr, P.d_near_src,         P.d_near_zoff,
+                                P.d_near_z32,  sysref(Q, qs, j * n), sysref(Q, qs, (j + 1) * n),
+                                sysd,          P.N,                  Ra};
+        near_batch_kernel<float2><<<ng, 128, 0, s>>>(na);
+      } else {
+        NearBatchArg<double2> na{P.d_leaf_rwg,  P.d_rwg_leafbox,      P.d_leaf_ptr,
+                                 P.d_near_sptr, P.d_near_src,         P.d_near_zoff,
+                                 P.d_near_z,    sysref(Q, qs, j * n), sysref(Q, qs, (j + 1) * n),
+                                 sysd,          P.N,                  Ra};
+        near_batch_kernel<double2><<<ng, 128, 0, s>>>(na);
+      }
       MLFMA_CUDA(cudaGetLastError());
       for (int q : list) st[q].near_products++;
       ops.orthogonalise(Ra, sysd, sysref(Q, qs, 0), sysref(Q, qs, (j + 1) * n), j + 1, hcol, hn);

@@ -14,6 +14,7 @@
 // onto the Bm that m2l of the same level has just written), so no clearing
 // pass (Code/ProcessMLFMM.h:14-28) is needed.
 #include <algorithm>
+#include <type_traits>
 
 #include "cplx.cuh"
 #include "plan.hpp"
@@ -24,29 +25,30 @@ namespace {
 
 constexpr int kThreads = 128;
 
-__global__ void __launch_bounds__(kThreads) agg_kernel(const double2* __restrict__ Vs,
-                                                       const int* __restrict__ leaf_ptr,
+// Aggregation: thread per (leaf box, direction), J and M from one pattern load.
+template <class C>
+__global__ void __launch_bounds__(kThreads) agg_kernel(const C* __restrict__ Vs, const int* __restrict__ leaf_ptr,
                                                        const int* __restrict__ leaf_rwg,
                                                        const double2* __restrict__ x, int N, int K,
-                                                       double2* __restrict__ S) {
+                                                       C* __restrict__ S) {
   const int kk = blockIdx.y * blockDim.x + threadIdx.x;
   const int b = blockIdx.x;
   if (kk >= K) return;
-  double2 acc[6];
+  C acc[6];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) acc[c] = c2(0.0, 0.0);
+  for (int c = 0; c < 6; ++c) acc[c] = Cx<C>::zero();
   const int r1 = leaf_ptr[b + 1];
   for (int r = leaf_ptr[b]; r < r1; ++r) {
     const int id = leaf_rwg[r];
-    const double2 xJ = x[id], xM = x[N + id];
+    const C xJ = Cx<C>::from(x[id]), xM = Cx<C>::from(x[N + id]);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const double2 v = Vs[(static_cast<size_t>(r) * 3 + c) * K + kk];
+      const C v = Vs[(static_cast<size_t>(r) * 3 + c) * K + kk];
       acc[c] = cfma(v, xJ, acc[c]);
       acc[3 + c] = cfma(v, xM, acc[3 + c]);
     }
   }
-  double2* out = S + static_cast<size_t>(b) * 6 * K + kk;
+  C* out = S + static_cast<size_t>(b) * 6 * K + kk;
 #pragma unroll
   for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * K] = acc[c];
 }
@@ -115,16 +117,17 @@ __global__ void __launch_bounds__(kThreads) agg_box_kernel(AggBoxArg a) {
   }
 }
 
+template <class C>
 struct UpArg {
-  const double2* Sc;   // child level patterns [Bc][6][Kc]
-  double2* Sp;         // parent level patterns [Bp][6][Kp]
+  const C* Sc;   // child level patterns [Bc][6][Kc]
+  C* Sp;               // parent level patterns [Bp][6][Kp]
   const int* child_begin;
   const int* octant;   // of child boxes
   const int* tidx;
   const double* lt;
   const int* pidx;
   const double* lp;
-  const double2* ph_up;
+  const C* ph_up;
   int Kp, nphp, Kc, nphc;
 };
 
@@ -132,7 +135,9 @@ struct UpArg {
 // separable interpolation of each child's pattern, times the child's shift
 // phase, summed over the children. One component per thread keeps the
 // register count low enough for the occupancy this gather needs.
-__global__ void __launch_bounds__(kThreads) up_kernel(UpArg a) {
+template <class C>
+__global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
+  using R = typename Cx<C>::real;
   const int kk = blockIdx.y * blockDim.x + threadIdx.x;
   const int b = blockIdx.x;
   const int c = blockIdx.z;
@@ -147,16 +152,16 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg a) {
     pi[i] = a.pidx[3 * p + i];
     wp[i] = a.lp[3 * p + i];
   }
-  double2 acc = c2(0.0, 0.0);
+  C acc = Cx<C>::zero();
   const int c1 = a.child_begin[b + 1];
   for (int ch = a.child_begin[b]; ch < c1; ++ch) {
-    const double2 e = a.ph_up[a.octant[ch] * a.Kp + kk];
-    const double2* sc = a.Sc + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
-    double2 v = c2(0.0, 0.0);
+    const C e = __ldg(a.ph_up + a.octant[ch] * a.Kp + kk);
+    const C* sc = a.Sc + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
+    C v = Cx<C>::zero();
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) v = cfmas(wt[i] * wp[j], __ldg(sc + ti[i] + pi[j]), v);
+      for (int j = 0; j < 3; ++j) v = cfmas(static_cast<R>(wt[i] * wp[j]), __ldg(sc + ti[i] + pi[j]), v);
     acc = cfma(e, v, acc);
   }
   a.Sp[(static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
@@ -166,7 +171,7 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg a) {
 // 6 components: the stencil (3 theta x 3 phi taps and weights) and the
 // child's shift phase are loaded once per child and applied to the 6
 // component rows, 54 independent loads per child in flight.
-__global__ void __launch_bounds__(kThreads) up6_kernel(UpArg a) {
+__global__ void __launch_bounds__(kThreads) up6_kernel(UpArg<double2> a) {
   const int kk = blockIdx.y * blockDim.x + threadIdx.x;
   const int b = blockIdx.x;
   if (kk >= a.Kp) return;
@@ -502,42 +507,45 @@ __global__ void __launch_bounds__(kM2lThreads, 2) m2l_oct_kernel(const __grid_co
 // repeats.
 constexpr int kWarpBoxes = 8;
 
+template <class C>
 struct M2lWarpSeg {
-  const double2* S;
-  double2* Bm;
-  const double2* tfw;
+  const C* S;
+  C* Bm;
+  const C* tfw;
   const int* far_ptr;
   const int* far_idx;
   const int* far_vec;
   int B, K, nchunk, cta_begin;
 };
+template <class C>
 struct M2lWarpArg {
-  M2lWarpSeg seg[kM2lMaxSeg];
+  M2lWarpSeg<C> seg[kM2lMaxSeg];
   int nseg;
 };
 
-__global__ void __launch_bounds__(32 * kWarpBoxes) m2l_warp_kernel(const __grid_constant__ M2lWarpArg a) {
+template <class C>
+__global__ void __launch_bounds__(32 * kWarpBoxes) m2l_warp_kernel(const __grid_constant__ M2lWarpArg<C> a) {
   int si = 0;
   while (si + 1 < a.nseg && static_cast<int>(blockIdx.x) >= a.seg[si + 1].cta_begin) ++si;
-  const M2lWarpSeg& g = a.seg[si];
+  const M2lWarpSeg<C>& g = a.seg[si];
   const int local = blockIdx.x - g.cta_begin;
   const int grp = local / g.nchunk;
   const int b = grp * kWarpBoxes + (threadIdx.x >> 5);
   const int k = (local - grp * g.nchunk) * 32 + (threadIdx.x & 31);
   const int K = g.K;
   if (b >= g.B || k >= K) return;
-  double2 acc[6];
+  C acc[6];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) acc[c] = c2(0.0, 0.0);
+  for (int c = 0; c < 6; ++c) acc[c] = Cx<C>::zero();
   const int e1 = g.far_ptr[b + 1];
   int e = g.far_ptr[b];
   for (; e + 1 < e1; e += 2) {
     const int s0 = __ldg(g.far_idx + e), s1 = __ldg(g.far_idx + e + 1);
-    const double2 t0 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e)) * K + k);
-    const double2 t1 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e + 1)) * K + k);
-    const double2* p0 = g.S + static_cast<size_t>(s0) * 6 * K + k;
-    const double2* p1 = g.S + static_cast<size_t>(s1) * 6 * K + k;
-    double2 v0[6], v1[6];
+    const C t0 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e)) * K + k);
+    const C t1 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e + 1)) * K + k);
+    const C* p0 = g.S + static_cast<size_t>(s0) * 6 * K + k;
+    const C* p1 = g.S + static_cast<size_t>(s1) * 6 * K + k;
+    C v0[6], v1[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       v0[c] = __ldg(p0 + static_cast<size_t>(c) * K);
@@ -548,12 +556,12 @@ __global__ void __launch_bounds__(32 * kWarpBoxes) m2l_warp_kernel(const __grid_
   }
   if (e < e1) {
     const int s0 = __ldg(g.far_idx + e);
-    const double2 t0 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e)) * K + k);
-    const double2* p0 = g.S + static_cast<size_t>(s0) * 6 * K + k;
+    const C t0 = __ldg(g.tfw + static_cast<size_t>(__ldg(g.far_vec + e)) * K + k);
+    const C* p0 = g.S + static_cast<size_t>(s0) * 6 * K + k;
 #pragma unroll
     for (int c = 0; c < 6; ++c) acc[c] = cfma(t0, __ldg(p0 + static_cast<size_t>(c) * K), acc[c]);
   }
-  double2* out = g.Bm + static_cast<size_t>(b) * 6 * K + k;
+  C* out = g.Bm + static_cast<size_t>(b) * 6 * K + k;
 #pragma unroll
   for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * K] = acc[c];
 }
@@ -590,12 +598,13 @@ __global__ void __launch_bounds__(kThreads) l2l_kernel(L2lArg a) {
   *out = cadd(*out, acc);
 }
 
+template <class C>
 struct L2lSepArg {
-  double2* Bm;           // child level (accumulated into)
-  const double2* Bp;     // parent level
+  C* Bm;                 // child level (accumulated into)
+  const C* Bp;     // parent level
   const int* parent;     // of child boxes
   const int* octant;     // of child boxes
-  const double2* ph_dn;  // parent level table [8][Kp]
+  const C* ph_dn;        // parent level table [8][Kp]
   const int* th_ptr;     // child theta row -> (parent theta row, Lagrange weight)
   const int* th_src;
   const double* th_w;
@@ -607,35 +616,42 @@ struct L2lSepArg {
 
 constexpr int kL2lBand = 2944;     // band entries in shared memory (46 KiB), all 6 components
 
-// Anterpolation (l2l), separable: one CTA per child box does all 6
-// components. The parent's incoming pattern is shifted to the child centre
+// child theta rows per band of the separable anterpolation
+__host__ __device__ __forceinline__ int l2l_band_rows(int ntc, int npp) {
+  return max(1, min(ntc, kL2lBand / (6 * npp)));
+}
+
+// Anterpolation (l2l), separable: one CTA per (child box, band of child theta
+// rows) does all 6 components. The parent's incoming pattern is shifted to the child centre
 // and spread onto the child grid by the transposed theta interpolation (into
 // a shared-memory band of child rows x parent phi columns x 6 components),
 // then by the transposed phi interpolation, and added to the child's Bm. The
 // reference's 9-tap weight of a (parent, child) direction pair is the
 // product of the two 1-D weights used here (Code/AlgoMLFMM.h:347-351).
-__global__ void __launch_bounds__(256) l2l_sep_kernel(L2lSepArg a) {
-  __shared__ double2 band[kL2lBand];
+template <class C>
+__global__ void __launch_bounds__(256) l2l_sep_kernel(L2lSepArg<C> a) {
+  using R = typename Cx<C>::real;
+  __shared__ C band[kL2lBand];
   const int b = blockIdx.x;
-  const int band_rows = max(1, min(a.ntc, kL2lBand / (6 * a.npp)));
+  const int band_rows = l2l_band_rows(a.ntc, a.npp);
   const int Kp = a.ntp * a.npp, Kc = a.ntc * a.npc;
-  const double2* ph = a.ph_dn + a.octant[b] * Kp;
-  const double2* bp = a.Bp + static_cast<size_t>(a.parent[b]) * 6 * Kp;
-  double2* out = a.Bm + static_cast<size_t>(b) * 6 * Kc;
-  for (int tc0 = 0; tc0 < a.ntc; tc0 += band_rows) {
+  const C* ph = a.ph_dn + a.octant[b] * Kp;
+  const C* bp = a.Bp + static_cast<size_t>(a.parent[b]) * 6 * Kp;
+  C* out = a.Bm + static_cast<size_t>(b) * 6 * Kc;
+  {
+    const int tc0 = blockIdx.y * band_rows;  // one band of child theta rows per CTA
     const int rows = min(band_rows, a.ntc - tc0);
     const int stride = rows * a.npp;
-    __syncthreads();
     for (int e = threadIdx.x; e < stride; e += blockDim.x) {
       const int r = e / a.npp, pp = e - r * a.npp;
       const int tc = tc0 + r;
-      double2 v[6];
+      C v[6];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) v[c] = c2(0.0, 0.0);
+      for (int c = 0; c < 6; ++c) v[c] = Cx<C>::zero();
       const int q1 = __ldg(a.th_ptr + tc + 1);
       for (int q = __ldg(a.th_ptr + tc); q < q1; ++q) {
         const int kp = __ldg(a.th_src + q) * a.npp + pp;
-        const double2 f = cscale(__ldg(ph + kp), __ldg(a.th_w + q));
+        const C f = cscale(__ldg(ph + kp), static_cast<R>(__ldg(a.th_w + q)));
 #pragma unroll
         for (int c = 0; c < 6; ++c) v[c] = cfma(f, __ldg(bp + static_cast<size_t>(c) * Kp + kp), v[c]);
       }
@@ -645,26 +661,27 @@ __global__ void __launch_bounds__(256) l2l_sep_kernel(L2lSepArg a) {
     __syncthreads();
     for (int e = threadIdx.x; e < rows * a.npc; e += blockDim.x) {
       const int r = e / a.npc, pc = e - r * a.npc;
-      double2 v[6];
+      C v[6];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) v[c] = c2(0.0, 0.0);
+      for (int c = 0; c < 6; ++c) v[c] = Cx<C>::zero();
       const int q1 = __ldg(a.ph_ptr + pc + 1);
       for (int q = __ldg(a.ph_ptr + pc); q < q1; ++q) {
-        const double w = __ldg(a.ph_w + q);
+        const R w = static_cast<R>(__ldg(a.ph_w + q));
         const int src = r * a.npp + __ldg(a.ph_src + q);
 #pragma unroll
         for (int c = 0; c < 6; ++c) v[c] = cfmas(w, band[c * stride + src], v[c]);
       }
-      double2* o = out + (tc0 + r) * a.npc + pc;
+      C* o = out + (tc0 + r) * a.npc + pc;
 #pragma unroll
       for (int c = 0; c < 6; ++c) o[static_cast<size_t>(c) * Kc] = cadd(o[static_cast<size_t>(c) * Kc], v[c]);
     }
   }
 }
 
+template <class C>
 struct LeafArg {
-  const double2* Vf[2];
-  const double2* Bm[2];
+  const C* Vf[2];
+  const C* Bm[2];
   const double* khat[2];
   int K[2];
   const int* leaf_rwg;
@@ -673,14 +690,15 @@ struct LeafArg {
   const int* near_sptr;
   const int* near_src;
   const long long* near_zoff;
-  const double2* near_z;
+  const C* near_z;
   const double2* x;
   double2* w;
   int N;
-  double2 c1, c2, etai;
+  C c1, c2, etai;
 };
 
-__device__ __forceinline__ double2 warp_sum(double2 v) {
+template <class C>
+__device__ __forceinline__ C warp_sum(C v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
@@ -690,29 +708,32 @@ __device__ __forceinline__ double2 warp_sum(double2 v) {
 }
 
 // One warp per RWG (leaf order).
-__global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg a) {
+template <class C>
+__global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg<C> a) {
+  using R = typename Cx<C>::real;
   const int lane = threadIdx.x & 31;
   const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   if (r >= a.N) return;
   const int id = a.leaf_rwg[r];
   const int b = a.rwg_box[id];
-  double2 res[8];  // L1J K1J L1M K1M L2J K2J L2M K2M
+  C res[8];  // L1J K1J L1M K1M L2J K2J L2M K2M
 #pragma unroll
   for (int m = 0; m < 2; ++m) {
     const int K = a.K[m];
-    const double2* V = a.Vf[m] + static_cast<size_t>(r) * 3 * K;
-    const double2* B = a.Bm[m] + static_cast<size_t>(b) * 6 * K;
+    const C* V = a.Vf[m] + static_cast<size_t>(r) * 3 * K;
+    const C* B = a.Bm[m] + static_cast<size_t>(b) * 6 * K;
     const double* kh = a.khat[m];
-    double2 LJ = c2(0, 0), KJ = c2(0, 0), LM = c2(0, 0), KM = c2(0, 0);
+    C LJ = Cx<C>::zero(), KJ = Cx<C>::zero(), LM = Cx<C>::zero(), KM = Cx<C>::zero();
+#pragma unroll 2
     for (int kk = lane; kk < K; kk += 32) {
-      const double2 v0 = V[kk], v1 = V[K + kk], v2 = V[2 * K + kk];
-      const double2 j0 = B[kk], j1 = B[K + kk], j2 = B[2 * K + kk];
-      const double2 m0 = B[3 * K + kk], m1 = B[4 * K + kk], m2 = B[5 * K + kk];
+      const C v0 = V[kk], v1 = V[K + kk], v2 = V[2 * K + kk];
+      const C j0 = B[kk], j1 = B[K + kk], j2 = B[2 * K + kk];
+      const C m0 = B[3 * K + kk], m1 = B[4 * K + kk], m2 = B[5 * K + kk];
       // (-khat) x V
-      const double ax = -kh[kk], ay = -kh[K + kk], az = -kh[2 * K + kk];
-      const double2 w0 = csub(cscale(v2, ay), cscale(v1, az));
-      const double2 w1 = csub(cscale(v0, az), cscale(v2, ax));
-      const double2 w2 = csub(cscale(v1, ax), cscale(v0, ay));
+      const R ax = static_cast<R>(-kh[kk]), ay = static_cast<R>(-kh[K + kk]), az = static_cast<R>(-kh[2 * K + kk]);
+      const C w0 = csub(cscale(v2, ay), cscale(v1, az));
+      const C w1 = csub(cscale(v0, az), cscale(v2, ax));
+      const C w2 = csub(cscale(v1, ax), cscale(v0, ay));
       LJ = cfma(v0, j0, cfma(v1, j1, cfma(v2, j2, LJ)));
       LM = cfma(v0, m0, cfma(v1, m1, cfma(v2, m2, LM)));
       KJ = cfma(w0, j0, cfma(w1, j1, cfma(w2, j2, KJ)));
@@ -726,12 +747,13 @@ __global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg a) {
   // near-field rows t and N + t
   const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
   const int tl = r - a.leaf_ptr[b];
-  const double2* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
-  double2 nJ = c2(0, 0), nM = c2(0, 0);
+  const C* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
+  C nJ = Cx<C>::zero(), nM = Cx<C>::zero();
+#pragma unroll 2
   for (int j = lane; j < ns; j += 32) {
     const int s = a.near_src[s0 + j];
-    const double2 xJ = a.x[s], xM = a.x[a.N + s];
-    const double2 z11 = Z[3 * j], z12 = Z[3 * j + 1], z22 = Z[3 * j + 2];
+    const C xJ = Cx<C>::from(a.x[s]), xM = Cx<C>::from(a.x[a.N + s]);
+    const C z11 = Z[3 * j], z12 = Z[3 * j + 1], z22 = Z[3 * j + 2];
     nJ = cfma(z11, xJ, cfma(z12, xM, nJ));
     nM = cfma(z22, xM, csub(nM, cmul(z12, xJ)));
   }
@@ -740,13 +762,13 @@ __global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg a) {
   if (lane == 0) {
     // w[t]   = c1 (L1J - K1M) + c2 (etai L2J - K2M) + near
     // w[N+t] = c1 (K1J + L1M) + c2 (K2J + L2M / etai) + near
-    const double2 L2M_eta = cdiv(res[6], a.etai);
-    double2 wj = cmul(a.c1, csub(res[0], res[3]));
+    const C L2M_eta = cdiv(res[6], a.etai);
+    C wj = cmul(a.c1, csub(res[0], res[3]));
     wj = cadd(wj, cmul(a.c2, csub(cmul(a.etai, res[4]), res[7])));
-    double2 wm = cmul(a.c1, cadd(res[1], res[2]));
+    C wm = cmul(a.c1, cadd(res[1], res[2]));
     wm = cadd(wm, cmul(a.c2, cadd(res[5], L2M_eta)));
-    a.w[id] = cadd(wj, nJ);
-    a.w[a.N + id] = cadd(wm, nM);
+    a.w[id] = Cx<C>::to64(cadd(wj, nJ));
+    a.w[a.N + id] = Cx<C>::to64(cadd(wm, nM));
   }
 }
 
@@ -756,9 +778,10 @@ __global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg a) {
 // each near-field entry once for a group of right-hand sides. Accumulation
 // orders are those of agg_box_kernel and leaf_out_kernel, so each right-hand
 // side of a batch gets the single apply's result.
+template <class C>
 struct AggBatchArg {
-  const double2* Vs[2];
-  double2* S[2][kBatchSlots];  // leaf-level S of each slot
+  const C* Vs[2];
+  C* S[2][kBatchSlots];  // leaf-level S of each slot
   int K[2];
   const int* leaf_ptr;
   const int* leaf_rwg;
@@ -767,34 +790,34 @@ struct AggBatchArg {
   int N, R;
 };
 
-template <int RB>
-__global__ void __launch_bounds__(kThreads) agg_batch_kernel(AggBatchArg a) {
+template <class C, int RB>
+__global__ void __launch_bounds__(kThreads) agg_batch_kernel(AggBatchArg<C> a) {
   const int b = blockIdx.x, m = blockIdx.y;
   const int j0 = blockIdx.z * RB, jn = min(RB, a.R - j0);
   const int K3 = 3 * a.K[m];
   const int r0 = a.leaf_ptr[b], r1 = a.leaf_ptr[b + 1];
-  const double2* V = a.Vs[m] + static_cast<size_t>(r0) * K3;
+  const C* V = a.Vs[m] + static_cast<size_t>(r0) * K3;
   for (int e = threadIdx.x; e < K3; e += blockDim.x) {
-    double2 aJ[RB], aM[RB];
+    C aJ[RB], aM[RB];
 #pragma unroll
-    for (int j = 0; j < RB; ++j) aJ[j] = aM[j] = c2(0.0, 0.0);
-    const double2* v = V + e;
+    for (int j = 0; j < RB; ++j) aJ[j] = aM[j] = Cx<C>::zero();
+    const C* v = V + e;
     for (int r = r0; r < r1; ++r, v += K3) {
       const int id = __ldg(a.leaf_rwg + r);
-      const double2 s = __ldg(v);
+      const C s = __ldg(v);
 #pragma unroll
       for (int j = 0; j < RB; ++j) {
         if (j < jn) {
           const double2* x = a.X + (j0 + j) * a.ldx;
-          aJ[j] = cfma(s, __ldg(x + id), aJ[j]);
-          aM[j] = cfma(s, __ldg(x + a.N + id), aM[j]);
+          aJ[j] = cfma(s, Cx<C>::from(__ldg(x + id)), aJ[j]);
+          aM[j] = cfma(s, Cx<C>::from(__ldg(x + a.N + id)), aM[j]);
         }
       }
     }
 #pragma unroll
     for (int j = 0; j < RB; ++j) {
       if (j < jn) {
-        double2* out = a.S[m][j0 + j] + static_cast<size_t>(b) * 2 * K3;
+        C* out = a.S[m][j0 + j] + static_cast<size_t>(b) * 2 * K3;
         out[e] = aJ[j];
         out[K3 + e] = aM[j];
       }
@@ -802,9 +825,10 @@ __global__ void __launch_bounds__(kThreads) agg_batch_kernel(AggBatchArg a) {
   }
 }
 
+template <class C>
 struct LeafBatchArg {
-  const double2* Vf[2];
-  const double2* Bm[2][kBatchSlots];  // leaf-level Bm of each slot
+  const C* Vf[2];
+  const C* Bm[2][kBatchSlots];  // leaf-level Bm of each slot
   const double* khat[2];
   int K[2];
   const int* leaf_rwg;
@@ -813,48 +837,49 @@ struct LeafBatchArg {
   const int* near_sptr;
   const int* near_src;
   const long long* near_zoff;
-  const double2* near_z;
+  const C* near_z;
   const double2* X;
   long long ldx;
   double2* W;
   long long ldw;
   int N, R;
-  double2 c1, c2, etai;
+  C c1, c2, etai;
 };
 
 // One warp per (RWG, group of RB right-hand sides).
-template <int RB>
-__global__ void __launch_bounds__(kThreads) leaf_out_batch_kernel(LeafBatchArg a) {
+template <class C, int RB>
+__global__ void __launch_bounds__(kThreads) leaf_out_batch_kernel(LeafBatchArg<C> a) {
+  using Rl = typename Cx<C>::real;
   const int lane = threadIdx.x & 31;
   const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   if (r >= a.N) return;
   const int j0 = blockIdx.y * RB, jn = min(RB, a.R - j0);
   const int id = a.leaf_rwg[r];
   const int b = a.rwg_box[id];
-  double2 wj[RB], wm[RB];
+  C wj[RB], wm[RB];
 #pragma unroll
   for (int m = 0; m < 2; ++m) {
     const int K = a.K[m];
-    const double2* V = a.Vf[m] + static_cast<size_t>(r) * 3 * K;
+    const C* V = a.Vf[m] + static_cast<size_t>(r) * 3 * K;
     const double* kh = a.khat[m];
-    double2 acc[RB][4];  // LJ KJ LM KM
+    C acc[RB][4];  // LJ KJ LM KM
 #pragma unroll
     for (int j = 0; j < RB; ++j)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[j][q] = c2(0.0, 0.0);
+      for (int q = 0; q < 4; ++q) acc[j][q] = Cx<C>::zero();
     for (int kk = lane; kk < K; kk += 32) {
-      const double2 v0 = V[kk], v1 = V[K + kk], v2 = V[2 * K + kk];
+      const C v0 = V[kk], v1 = V[K + kk], v2 = V[2 * K + kk];
       // (-khat) x V
-      const double ax = -kh[kk], ay = -kh[K + kk], az = -kh[2 * K + kk];
-      const double2 w0 = csub(cscale(v2, ay), cscale(v1, az));
-      const double2 w1 = csub(cscale(v0, az), cscale(v2, ax));
-      const double2 w2 = csub(cscale(v1, ax), cscale(v0, ay));
+      const Rl ax = static_cast<Rl>(-kh[kk]), ay = static_cast<Rl>(-kh[K + kk]), az = static_cast<Rl>(-kh[2 * K + kk]);
+      const C w0 = csub(cscale(v2, ay), cscale(v1, az));
+      const C w1 = csub(cscale(v0, az), cscale(v2, ax));
+      const C w2 = csub(cscale(v1, ax), cscale(v0, ay));
 #pragma unroll
       for (int j = 0; j < RB; ++j) {
         if (j < jn) {
-          const double2* B = a.Bm[m][j0 + j] + static_cast<size_t>(b) * 6 * K;
-          const double2 b0 = B[kk], b1 = B[K + kk], b2 = B[2 * K + kk];
-          const double2 m0 = B[3 * K + kk], m1 = B[4 * K + kk], m2 = B[5 * K + kk];
+          const C* B = a.Bm[m][j0 + j] + static_cast<size_t>(b) * 6 * K;
+          const C b0 = B[kk], b1 = B[K + kk], b2 = B[2 * K + kk];
+          const C m0 = B[3 * K + kk], m1 = B[4 * K + kk], m2 = B[5 * K + kk];
           acc[j][0] = cfma(v0, b0, cfma(v1, b1, cfma(v2, b2, acc[j][0])));
           acc[j][2] = cfma(v0, m0, cfma(v1, m1, cfma(v2, m2, acc[j][2])));
           acc[j][1] = cfma(w0, b0, cfma(w1, b1, cfma(w2, b2, acc[j][1])));
@@ -864,8 +889,8 @@ __global__ void __launch_bounds__(kThreads) leaf_out_batch_kernel(LeafBatchArg a
     }
 #pragma unroll
     for (int j = 0; j < RB; ++j) {
-      const double2 LJ = warp_sum(acc[j][0]), KJ = warp_sum(acc[j][1]);
-      const double2 LM = warp_sum(acc[j][2]), KM = warp_sum(acc[j][3]);
+      const C LJ = warp_sum(acc[j][0]), KJ = warp_sum(acc[j][1]);
+      const C LM = warp_sum(acc[j][2]), KM = warp_sum(acc[j][3]);
       if (m == 0) {
         wj[j] = cmul(a.c1, csub(LJ, KM));
         wm[j] = cmul(a.c1, cadd(KJ, LM));
@@ -877,18 +902,18 @@ __global__ void __launch_bounds__(kThreads) leaf_out_batch_kernel(LeafBatchArg a
   }
   const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
   const int tl = r - a.leaf_ptr[b];
-  const double2* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
-  double2 nJ[RB], nM[RB];
+  const C* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
+  C nJ[RB], nM[RB];
 #pragma unroll
-  for (int j = 0; j < RB; ++j) nJ[j] = nM[j] = c2(0.0, 0.0);
+  for (int j = 0; j < RB; ++j) nJ[j] = nM[j] = Cx<C>::zero();
   for (int q = lane; q < ns; q += 32) {
     const int src = a.near_src[s0 + q];
-    const double2 z11 = Z[3 * q], z12 = Z[3 * q + 1], z22 = Z[3 * q + 2];
+    const C z11 = Z[3 * q], z12 = Z[3 * q + 1], z22 = Z[3 * q + 2];
 #pragma unroll
     for (int j = 0; j < RB; ++j) {
       if (j < jn) {
         const double2* x = a.X + (j0 + j) * a.ldx;
-        const double2 xJ = x[src], xM = x[a.N + src];
+        const C xJ = Cx<C>::from(x[src]), xM = Cx<C>::from(x[a.N + src]);
         nJ[j] = cfma(z11, xJ, cfma(z12, xM, nJ[j]));
         nM[j] = cfma(z22, xM, csub(nM[j], cmul(z12, xJ)));
       }
@@ -896,11 +921,11 @@ __global__ void __launch_bounds__(kThreads) leaf_out_batch_kernel(LeafBatchArg a
   }
 #pragma unroll
   for (int j = 0; j < RB; ++j) {
-    const double2 sJ = warp_sum(nJ[j]), sM = warp_sum(nM[j]);
+    const C sJ = warp_sum(nJ[j]), sM = warp_sum(nM[j]);
     if (lane == 0 && j < jn) {
       double2* w = a.W + (j0 + j) * a.ldw;
-      w[id] = cadd(wj[j], sJ);
-      w[a.N + id] = cadd(wm[j], sM);
+      w[id] = Cx<C>::to64(cadd(wj[j], sJ));
+      w[a.N + id] = Cx<C>::to64(cadd(wm[j], sM));
     }
   }
 }
@@ -923,8 +948,8 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
     const MediumLevel& cm = P.ml[m][l + 1];
     const double2* Sc = level_S(P, m, l + 1, v);
     if (P.tuning.up_variant == 2) {
-      UpArg a{Sc, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
-              pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
+      UpArg<double2> a{Sc, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
+                       pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
       up6_kernel<<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads), kThreads, 0, s>>>(a);
     } else if (P.tuning.up_variant == 1 && pm.up_rows > 0) {
       UpSepArg a{Sc,    pm.S,     P.lv[l].child_begin, P.lv[l + 1].octant, pm.pidx,
@@ -933,10 +958,10 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
                  pm.up_rows};
       up_sep_kernel<<<dim3(P.lv[l].B, 6, pm.up_nband), 256, 0, s>>>(a);
     } else {
-      UpArg a{Sc, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
-              pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
+      UpArg<double2> a{Sc, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
+                       pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
       dim3 gu(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6);
-      up_kernel<<<gu, kThreads, 0, s>>>(a);
+      up_kernel<double2><<<gu, kThreads, 0, s>>>(a);
     }
   }
 }
@@ -946,16 +971,16 @@ void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
   const int L = P.maxL;
   if (P.tuning.m2l_variant == 3) {
     if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
-    M2lWarpArg a{};
+    M2lWarpArg<double2> a{};
     int ctas = 0;
     for (int l = 2; l <= L; ++l) {
       const MediumLevel& cm = P.ml[m][l];
-      M2lWarpSeg& g = a.seg[a.nseg++];
-      g = M2lWarpSeg{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, P.lv[l].far_ptr, P.lv[l].far_idx,
+      M2lWarpSeg<double2>& g = a.seg[a.nseg++];
+      g = M2lWarpSeg<double2>{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, P.lv[l].far_ptr, P.lv[l].far_idx,
                      P.lv[l].far_vec, P.lv[l].B, cm.K, (cm.K + 31) / 32, ctas};
       ctas += ((P.lv[l].B + kWarpBoxes - 1) / kWarpBoxes) * g.nchunk;
     }
-    m2l_warp_kernel<<<ctas, 32 * kWarpBoxes, 0, s>>>(a);
+    m2l_warp_kernel<double2><<<ctas, 32 * kWarpBoxes, 0, s>>>(a);
     return;
   }
   if (P.tuning.m2l_variant == 2) {
@@ -998,10 +1023,11 @@ void launch_l2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
     const MediumLevel& pm = P.ml[m][l - 1];
     double2* Bc = level_B(P, m, l, v);
     if (P.tuning.l2l_variant == 1 && 6 * pm.nph <= kL2lBand) {
-      L2lSepArg b{Bc,         pm.Bm,    P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.thT_ptr,
+      L2lSepArg<double2> b{Bc,         pm.Bm,    P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.thT_ptr,
                   cm.thT_src, cm.thT_w, cm.phT_ptr,     cm.phT_src,     cm.phT_w, cm.nth,
                   cm.nph,     pm.nth,   pm.nph};
-      l2l_sep_kernel<<<P.lv[l].B, 256, 0, s>>>(b);
+      const int nband = (cm.nth + l2l_band_rows(cm.nth, pm.nph) - 1) / l2l_band_rows(cm.nth, pm.nph);
+      l2l_sep_kernel<double2><<<dim3(P.lv[l].B, nband), 256, 0, s>>>(b);
     } else {
       L2lArg b{Bc, pm.Bm, P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.tr_ptr, cm.tr_kp, cm.tr_w, cm.K, pm.K};
       dim3 gl(P.lv[l].B, (cm.K + kThreads - 1) / kThreads, 6);
@@ -1012,19 +1038,20 @@ void launch_l2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
 
 template <class Arg>
 void fill_leaf_common(const Plan& P, Arg& a) {
+  using C = std::remove_reference_t<decltype(a.c1)>;
   a.leaf_rwg = P.d_leaf_rwg;
   a.rwg_box = P.d_rwg_leafbox;
   a.leaf_ptr = P.d_leaf_ptr;
   a.near_sptr = P.d_near_sptr;
   a.near_src = P.d_near_src;
   a.near_zoff = P.d_near_zoff;
-  a.near_z = P.d_near_z;
+  a.near_z = Store<C>::near_z(P);
   a.N = P.N;
   const cplx c1 = P.k1 * P.k1 / (16.0 * kPi * kPi);
   const cplx c2v = P.k2 * P.k2 / (16.0 * kPi * kPi);
-  a.c1 = c2(c1.real(), c1.imag());
-  a.c2 = c2(c2v.real(), c2v.imag());
-  a.etai = c2(P.etai.real(), P.etai.imag());
+  a.c1 = Cx<C>::from(c2(c1.real(), c1.imag()));
+  a.c2 = Cx<C>::from(c2(c2v.real(), c2v.imag()));
+  a.etai = Cx<C>::from(c2(P.etai.real(), P.etai.imag()));
 }
 
 cudaEvent_t* profiler_events(Plan& P, cudaStream_t s) {
@@ -1038,6 +1065,108 @@ cudaEvent_t* profiler_events(Plan& P, cudaStream_t s) {
   cudaEvent_t* ev = P.prof.sets[P.prof.used++].data();
   MLFMA_CUDA(cudaEventRecord(ev[0], s));
   return ev;
+}
+
+// The tree passes of medium m with fixed kernel choices (interpolation 0,
+// translation 3, anterpolation 1) for either storage type; leafS / leafB are
+// the leaf-level arrays (the plan's own or one batch slot).
+template <class C>
+void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s) {
+  const int L = P.maxL;
+  auto S_at = [&](int l) -> C* { return l == L ? leafS : Store<C>::S(P.ml[m][l]); };
+  auto B_at = [&](int l) -> C* { return l == L ? leafB : Store<C>::Bm(P.ml[m][l]); };
+  for (int l = L - 1; l >= 2; --l) {
+    const MediumLevel& pm = P.ml[m][l];
+    const MediumLevel& cm = P.ml[m][l + 1];
+    UpArg<C> a{S_at(l + 1), S_at(l), P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
+               Store<C>::ph_up(pm), pm.K, pm.nph, cm.K, cm.nph};
+    up_kernel<C><<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6), kThreads, 0, s>>>(a);
+  }
+  if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+  M2lWarpArg<C> t{};
+  int ctas = 0;
+  for (int l = 2; l <= L; ++l) {
+    const MediumLevel& cm = P.ml[m][l];
+    M2lWarpSeg<C>& g = t.seg[t.nseg++];
+    g = M2lWarpSeg<C>{S_at(l),         B_at(l), Store<C>::tfw(cm), P.lv[l].far_ptr, P.lv[l].far_idx, P.lv[l].far_vec,
+                      P.lv[l].B,       cm.K,    (cm.K + 31) / 32,   ctas};
+    ctas += ((P.lv[l].B + kWarpBoxes - 1) / kWarpBoxes) * g.nchunk;
+  }
+  m2l_warp_kernel<C><<<ctas, 32 * kWarpBoxes, 0, s>>>(t);
+  for (int l = 3; l <= L; ++l) {
+    const MediumLevel& cm = P.ml[m][l];
+    const MediumLevel& pm = P.ml[m][l - 1];
+    if (6 * pm.nph > kL2lBand) throw std::runtime_error("anterpolation band: phi grid too large for this precision");
+    L2lSepArg<C> b{B_at(l),    B_at(l - 1), P.lv[l].parent, P.lv[l].octant, Store<C>::ph_dn(pm), cm.thT_ptr,
+                   cm.thT_src, cm.thT_w,    cm.phT_ptr,     cm.phT_src,     cm.phT_w,            cm.nth,
+                   cm.nph,     pm.nth,      pm.nph};
+    const int nband = (cm.nth + l2l_band_rows(cm.nth, pm.nph) - 1) / l2l_band_rows(cm.nth, pm.nph);
+    l2l_sep_kernel<C><<<dim3(P.lv[l].B, nband), 256, 0, s>>>(b);
+  }
+}
+
+template <class C>
+void apply_fixed(Plan& P, const double2* x, double2* w, cudaStream_t s) {
+  const int L = P.maxL;
+  LeafArg<C> a{};
+  for (int m = 0; m < 2; ++m) {
+    const MediumLevel& leaf = P.ml[m][L];
+    agg_kernel<C><<<dim3(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+        Store<C>::Vs(P, m), P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, Store<C>::S(leaf));
+    tree_pass_fixed<C>(P, m, Store<C>::S(leaf), Store<C>::Bm(leaf), s);
+    a.Vf[m] = Store<C>::Vf(P, m);
+    a.Bm[m] = Store<C>::Bm(leaf);
+    a.khat[m] = leaf.khat;
+    a.K[m] = leaf.K;
+  }
+  fill_leaf_common(P, a);
+  a.x = x;
+  a.w = w;
+  const int warps = kThreads / 32;
+  leaf_out_kernel<C><<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
+  MLFMA_CUDA(cudaGetLastError());
+}
+
+template <class C>
+void apply_batch_fixed(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw, cudaStream_t s) {
+  const int L = P.maxL;
+  if (P.batch_cap < std::min(R, kBatchSlots)) throw std::runtime_error("batched apply: slots not reserved");
+  constexpr int kAggRB = 8, kLeafRB = 4;
+  for (int g0 = 0; g0 < R; g0 += kBatchSlots) {
+    const int rn = std::min(kBatchSlots, R - g0);
+    AggBatchArg<C> ag{};
+    for (int m = 0; m < 2; ++m) {
+      ag.Vs[m] = Store<C>::Vs(P, m);
+      ag.K[m] = P.ml[m][L].K;
+      for (int j = 0; j < rn; ++j) ag.S[m][j] = Store<C>::bS(P, m, j);
+    }
+    ag.leaf_ptr = P.d_leaf_ptr;
+    ag.leaf_rwg = P.d_leaf_rwg;
+    ag.X = X + g0 * ldx;
+    ag.ldx = ldx;
+    ag.N = P.N;
+    ag.R = rn;
+    agg_batch_kernel<C, kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
+    for (int j = 0; j < rn; ++j)
+      for (int m = 0; m < 2; ++m) tree_pass_fixed<C>(P, m, Store<C>::bS(P, m, j), Store<C>::bB(P, m, j), s);
+    LeafBatchArg<C> lb{};
+    for (int m = 0; m < 2; ++m) {
+      lb.Vf[m] = Store<C>::Vf(P, m);
+      lb.khat[m] = P.ml[m][L].khat;
+      lb.K[m] = P.ml[m][L].K;
+      for (int j = 0; j < rn; ++j) lb.Bm[m][j] = Store<C>::bB(P, m, j);
+    }
+    fill_leaf_common(P, lb);
+    lb.X = X + g0 * ldx;
+    lb.ldx = ldx;
+    lb.W = W + g0 * ldw;
+    lb.ldw = ldw;
+    lb.R = rn;
+    const int warps = kThreads / 32;
+    leaf_out_batch_kernel<C, kLeafRB>
+        <<<dim3((P.N + warps - 1) / warps, (rn + kLeafRB - 1) / kLeafRB), kThreads, 0, s>>>(lb);
+    MLFMA_CUDA(cudaGetLastError());
+  }
 }
 
 }  // namespace
@@ -1062,7 +1191,7 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
     const MediumLevel& leaf = P.ml[m][L];
     if (P.tuning.agg_variant == 0) {
       dim3 g(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads);
-      agg_kernel<<<g, kThreads, 0, s>>>(P.d_Vs[m], P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, leaf.S);
+      agg_kernel<double2><<<g, kThreads, 0, s>>>(P.d_Vs[m], P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, leaf.S);
     }
     if (ev) MLFMA_CUDA(cudaEventRecord(ev[1 + 4 * m], s));
     const LeafView v{leaf.S, leaf.Bm};
@@ -1073,7 +1202,7 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
     launch_l2l(P, m, v, s);
     if (ev) MLFMA_CUDA(cudaEventRecord(ev[4 + 4 * m], s));
   }
-  LeafArg a{};
+  LeafArg<double2> a{};
   for (int m = 0; m < 2; ++m) {
     a.Vf[m] = P.d_Vf[m];
     a.Bm[m] = P.ml[m][L].Bm;
@@ -1084,7 +1213,7 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   a.x = x;
   a.w = w;
   const int warps = kThreads / 32;
-  leaf_out_kernel<<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
+  leaf_out_kernel<double2><<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
   MLFMA_CUDA(cudaGetLastError());
   if (ev) MLFMA_CUDA(cudaEventRecord(ev[9], s));
 }
@@ -1097,6 +1226,10 @@ void reserve_batch(Plan& P, int R) {
       const size_t cnt = static_cast<size_t>(P.lv[L].B) * 6 * P.ml[m][L].K;
       P.bS[m].push_back(P.alloc<double2>(cnt));
       P.bB[m].push_back(P.alloc<double2>(cnt));
+      if (P.precision == 1) {
+        P.bS32[m].push_back(P.alloc<float2>(cnt));
+        P.bB32[m].push_back(P.alloc<float2>(cnt));
+      }
     }
     ++P.batch_cap;
   }
@@ -1108,7 +1241,7 @@ void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2
   constexpr int kAggRB = 8, kLeafRB = 4;
   for (int g0 = 0; g0 < R; g0 += kBatchSlots) {
     const int rn = std::min(kBatchSlots, R - g0);
-    AggBatchArg ag{};
+    AggBatchArg<double2> ag{};
     for (int m = 0; m < 2; ++m) {
       ag.Vs[m] = P.d_Vs[m];
       ag.K[m] = P.ml[m][L].K;
@@ -1120,7 +1253,7 @@ void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2
     ag.ldx = ldx;
     ag.N = P.N;
     ag.R = rn;
-    agg_batch_kernel<kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
+    agg_batch_kernel<double2, kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
     for (int j = 0; j < rn; ++j)
       for (int m = 0; m < 2; ++m) {
         const LeafView v{P.bS[m][j], P.bB[m][j]};
@@ -1128,7 +1261,7 @@ void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2
         launch_m2l(P, m, v, s);
         launch_l2l(P, m, v, s);
       }
-    LeafBatchArg lb{};
+    LeafBatchArg<double2> lb{};
     for (int m = 0; m < 2; ++m) {
       lb.Vf[m] = P.d_Vf[m];
       lb.khat[m] = P.ml[m][L].khat;
@@ -1142,9 +1275,20 @@ void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2
     lb.ldw = ldw;
     lb.R = rn;
     const int warps = kThreads / 32;
-    leaf_out_batch_kernel<kLeafRB><<<dim3((P.N + warps - 1) / warps, (rn + kLeafRB - 1) / kLeafRB), kThreads, 0, s>>>(lb);
+    leaf_out_batch_kernel<double2, kLeafRB><<<dim3((P.N + warps - 1) / warps, (rn + kLeafRB - 1) / kLeafRB), kThreads, 0, s>>>(lb);
     MLFMA_CUDA(cudaGetLastError());
   }
+}
+
+void apply_mixed_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
+  if (P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
+  apply_fixed<float2>(P, x, w, s);
+}
+
+void apply_batch_mixed_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw,
+                              cudaStream_t s) {
+  if (P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
+  apply_batch_fixed<float2>(P, R, X, ldx, W, ldw, s);
 }
 
 }  // namespace mlfma

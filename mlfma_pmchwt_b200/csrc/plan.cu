@@ -60,6 +60,8 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   P->device = prm.device;
   P->verbose = prm.verbose;
   P->tf_complex_argument = prm.tf_complex_argument;
+  if (prm.precision != 0 && prm.precision != 1) throw std::invalid_argument("precision must be 0 (FP64) or 1 (mixed)");
+  P->precision = prm.precision;
   P->mesh = std::move(mesh);
   if (!(prm.freq > 0) || !(prm.leaf_coeff > 0)) throw std::invalid_argument("freq and leaf_coeff must be positive");
   if (!quad_rule(prm.gauss, P->quad)) throw std::invalid_argument("unsupported triangle rule");
@@ -374,6 +376,31 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   }
   P->d_x = P->alloc<double2>(2 * static_cast<size_t>(P->N));
   P->d_w = P->alloc<double2>(2 * static_cast<size_t>(P->N));
+  // complex64 copies of the operator's tables and its workspaces
+  if (P->precision == 1) {
+    auto copy32 = [&](const double2* src, size_t n) {
+      float2* d = P->alloc<float2>(n);
+      to_c64(src, d, n, s);
+      return d;
+    };
+    for (int m = 0; m < 2; ++m) {
+      const size_t np = static_cast<size_t>(P->N) * 3 * P->ml[m][L].K;
+      P->d_Vs32[m] = copy32(P->d_Vs[m], np);
+      P->d_Vf32[m] = copy32(P->d_Vf[m], np);
+      for (int l = 2; l <= L; ++l) {
+        MediumLevel& M = P->ml[m][l];
+        const size_t nb = static_cast<size_t>(P->lv[l].B) * 6 * M.K;
+        M.S32 = P->alloc<float2>(nb);
+        M.Bm32 = P->alloc<float2>(nb);
+        M.tfw32 = copy32(M.tfw, static_cast<size_t>(std::max(M.nvec, 1)) * M.K);
+        if (l < L) {
+          M.ph_up32 = copy32(M.ph_up, 8 * static_cast<size_t>(M.K));
+          M.ph_dn32 = copy32(M.ph_dn, 8 * static_cast<size_t>(M.K));
+        }
+      }
+    }
+    P->d_near_z32 = copy32(P->d_near_z, 3 * static_cast<size_t>(std::max<long long>(P->near_pairs, 1)));
+  }
   MLFMA_CUDA(cudaStreamSynchronize(s));
   P->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (P->verbose) {

@@ -30,6 +30,8 @@ struct MediumLevel {
   double2* S = nullptr;
   double2* Bm = nullptr;
   double2* tfw = nullptr;      // [nvec][K], weights folded in
+  // complex64 copies for the mixed-precision operator (precision = mixed only)
+  float2 *S32 = nullptr, *Bm32 = nullptr, *tfw32 = nullptr, *ph_up32 = nullptr, *ph_dn32 = nullptr;
   int nvec = 0;
   int* off2vec = nullptr;      // [343] -> vec index or -1
   double* khat = nullptr;      // [3][K] (x row, y row, z row)
@@ -121,6 +123,7 @@ struct Plan {
   int device = 0;
   int verbose = 0;
   int tf_complex_argument = 0;
+  int precision = 0;                // 0: FP64 operator; 1: also the complex64 operator
   cplx k1, k2, eta1, eta2, etai, epsr, mur;
   double lambda = 0.0, freq = 0.0;
   double setup_seconds = 0.0;
@@ -146,6 +149,8 @@ struct Plan {
   double* d_leaf_center = nullptr;  // [3 * Bleaf]
   double2* d_Vs[2] = {nullptr, nullptr};   // radiation patterns [N][3][K]
   double2* d_Vf[2] = {nullptr, nullptr};   // receive patterns
+  float2* d_Vs32[2] = {nullptr, nullptr};  // complex64 copies (precision = mixed)
+  float2* d_Vf32[2] = {nullptr, nullptr};
   // ---- near field
   std::vector<long long> h_near_zoff;      // per leaf box, offset of its block (pairs)
   std::vector<int> h_near_sptr;            // per leaf box, offset into source list
@@ -154,6 +159,7 @@ struct Plan {
   int* d_near_src = nullptr;        // concatenated source RWG ids per box
   long long* d_near_zoff = nullptr; // [Bleaf+1]
   double2* d_near_z = nullptr;      // [pairs][3]
+  float2* d_near_z32 = nullptr;     // complex64 copy (precision = mixed)
   long long near_pairs = 0;
   // ---- vectors
   double2* d_x = nullptr;           // staging for host-pointer apply
@@ -162,6 +168,7 @@ struct Plan {
   // (levels above the leaf are shared: the slots pass through them in turn)
   int batch_cap = 0;
   std::vector<double2*> bS[2], bB[2];
+  std::vector<float2*> bS32[2], bB32[2];
   double2* d_xb = nullptr;          // staging for host-pointer batched apply
   double2* d_wb = nullptr;
   int xb_cap = 0;
@@ -212,8 +219,43 @@ struct PlanParams {
   // lossy (complex) k (Code/AlgoMLFMM.h:262-265). 1: h2_l(kR) with the
   // complex argument, consistent with the complex-k shifts and near field.
   int tf_complex_argument = 0;
+  // 0: FP64 operator only. 1: also complex64 copies of the patterns, transfer
+  // factors, shift phases, near field and workspaces, for the mixed-precision
+  // apply and solves.
+  int precision = 0;
 };
 std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& p);
+
+// The arrays of one storage precision: double2 (the FP64 operator) or float2
+// (the complex64 copies), for code templated over the kernels' storage type.
+template <class C>
+struct Store;
+template <>
+struct Store<double2> {
+  static double2* S(const MediumLevel& M) { return M.S; }
+  static double2* Bm(const MediumLevel& M) { return M.Bm; }
+  static const double2* tfw(const MediumLevel& M) { return M.tfw; }
+  static const double2* ph_up(const MediumLevel& M) { return M.ph_up; }
+  static const double2* ph_dn(const MediumLevel& M) { return M.ph_dn; }
+  static const double2* Vs(const Plan& P, int m) { return P.d_Vs[m]; }
+  static const double2* Vf(const Plan& P, int m) { return P.d_Vf[m]; }
+  static const double2* near_z(const Plan& P) { return P.d_near_z; }
+  static double2* bS(const Plan& P, int m, int j) { return P.bS[m][j]; }
+  static double2* bB(const Plan& P, int m, int j) { return P.bB[m][j]; }
+};
+template <>
+struct Store<float2> {
+  static float2* S(const MediumLevel& M) { return M.S32; }
+  static float2* Bm(const MediumLevel& M) { return M.Bm32; }
+  static const float2* tfw(const MediumLevel& M) { return M.tfw32; }
+  static const float2* ph_up(const MediumLevel& M) { return M.ph_up32; }
+  static const float2* ph_dn(const MediumLevel& M) { return M.ph_dn32; }
+  static const float2* Vs(const Plan& P, int m) { return P.d_Vs32[m]; }
+  static const float2* Vf(const Plan& P, int m) { return P.d_Vf32[m]; }
+  static const float2* near_z(const Plan& P) { return P.d_near_z32; }
+  static float2* bS(const Plan& P, int m, int j) { return P.bS32[m][j]; }
+  static float2* bB(const Plan& P, int m, int j) { return P.bB32[m][j]; }
+};
 
 // Device work (setup_kernels.cu / matvec_kernels.cu)
 void launch_patterns(Plan& P, int medium, cudaStream_t s);
@@ -227,6 +269,14 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s);
 constexpr int kBatchSlots = 16;
 void reserve_batch(Plan& P, int R);  // allocates the leaf-level arrays of min(R, kBatchSlots) slots
 void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw, cudaStream_t s);
+// The complex64 operator (precision = mixed plans): complex128 x and w, every
+// table and workspace in complex64, FP32 arithmetic. Fixed kernel choices:
+// aggregation 0, interpolation 0, translation 3, anterpolation 1.
+void apply_mixed_device(Plan& P, const double2* x, double2* w, cudaStream_t s);
+void apply_batch_mixed_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw,
+                              cudaStream_t s);
+// complex128 -> complex64 copy on the device
+void to_c64(const double2* src, float2* dst, size_t n, cudaStream_t s);
 int read_stage_times(Plan& P, double out[kStages]);
 
 }  // namespace mlfma

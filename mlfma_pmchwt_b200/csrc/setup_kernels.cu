@@ -4,6 +4,7 @@
 //  * near-field PMCHWT entries from the RWG L and K operators with the
 //    analytic extraction of the 1/R and 1/R^3 parts on coincident triangles
 //    (Code/Operator.h:10-1046, assembled as Code/Zmartix.h:541-643).
+#include <algorithm>
 #include "cplx.cuh"
 #include "plan.hpp"
 
@@ -424,6 +425,20 @@ GeomArg geom_arg(const Plan& P) {
 }
 
 }  // namespace
+
+namespace {
+__global__ void to_c64_kernel(const double2* __restrict__ src, float2* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    dst[i] = make_float2(static_cast<float>(src[i].x), static_cast<float>(src[i].y));
+}
+}  // namespace
+
+void to_c64(const double2* src, float2* dst, size_t n, cudaStream_t s) {
+  const int blocks = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16));
+  to_c64_kernel<<<std::max(blocks, 1), 256, 0, s>>>(src, dst, n);
+  MLFMA_CUDA(cudaGetLastError());
+}
 
 void launch_patterns(Plan& P, int medium, cudaStream_t s) {
   const MediumLevel& M = P.ml[medium][P.maxL];

@@ -22,8 +22,18 @@ bool gmres_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, dou
 
 // Flexible GMRES(mr) whose right preconditioner is inner_its GMRES steps on
 // the near-field matrix alone (fgmres.cu); inner_its = 0 gives plain GMRES.
+// prec 1: the operator and near field are the plan's complex64 copies (the
+// Krylov vectors and Gram-Schmidt stay complex128).
 bool fgmres_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, double tol_abs, double tol_rel,
-                  int inner_its, SolveStats& st, std::vector<double>& history);
+                  int inner_its, SolveStats& st, std::vector<double>& history, int prec = 0);
+
+// Mixed precision: FP64 iterative refinement (mixed.cu). Each step solves the
+// correction equation A d = r with the complex64 operator (fgmres_solve,
+// prec 1) to a relative tolerance that aims at tol_rel, then recomputes the
+// residual r = b - A x with the FP64 operator. history: the FP64 relative
+// residual after each refinement step.
+bool mixed_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, double tol_abs, double tol_rel,
+                 int inner_its, int refine_max, SolveStats& st, std::vector<double>& history);
 
 // Lockstep FGMRES of R systems (fgmres_batch.cu): x, rhs host complex128
 // [R][2N]; per system the iteration of fgmres_solve, with every operator
@@ -31,10 +41,16 @@ bool fgmres_solve(Plan& P, double* x, const double* rhs, int itr_max, int mr, do
 // Returns the converged flag of each system.
 std::vector<char> fgmres_batch_solve(Plan& P, int R, double* x, const double* rhs, int itr_max, int mr,
                                      double tol_abs, double tol_rel, int inner_its, std::vector<SolveStats>& st,
-                                     std::vector<std::vector<double>>& hist, double& seconds);
+                                     std::vector<std::vector<double>>& hist, double& seconds, int prec = 0);
+
+// mixed_solve for R systems: FP64 residuals by batched applies, corrections
+// by fgmres_batch_solve with the complex64 operator.
+std::vector<char> mixed_batch_solve(Plan& P, int R, double* x, const double* rhs, int itr_max, int mr,
+                                    double tol_abs, double tol_rel, int inner_its, int refine_max,
+                                    std::vector<SolveStats>& st, double& seconds);
 
 // w = Z_near x on device vectors (complex128 [2N]).
-void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s);
+void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s, int prec = 0);
 
 void rhs_pmchwt(Plan& P, const double kinc[3], const double einc[3], const double hinc[3], double* V);
 

@@ -1,0 +1,70 @@
+"""Mixed precision: the complex64 operator against the FP64 one, and FP64
+iterative refinement around complex64 FGMRES reaching FP64 tolerances that
+the complex64 operator alone cannot (single and lockstep multi-RHS)."""
+import numpy as np
+import pytest
+
+from conftest import FREQ, needs_lib, needs_oracle, rel
+
+pytestmark = [pytest.mark.gpu, needs_lib]
+
+_ops = {}
+
+
+def mixed_op(case_files, name):
+    from mlfma_pmchwt_b200 import MLFMM
+    if name not in _ops:
+        m, p, eps, leaf = case_files[name]
+        _ops[name] = MLFMM(m, freq=FREQ, eps_r=eps, leaf_coeff=leaf, device=0, precision="mixed")
+    return _ops[name]
+
+
+@pytest.mark.parametrize("name", ["sphere_s3_lossy", "ellipsoid_s3", "sphere_s4_deep"])
+def test_complex64_operator_close_to_fp64(case_files, name):
+    from mlfma_pmchwt_b200 import mesh as M
+    op = mixed_op(case_files, name)
+    for seed in (0, 5):
+        x = M.unit_disk_vector(op.n, seed)
+        e = rel(op.apply_ax_mixed(x), op.apply_ax(x))
+        assert 1e-9 < e < 1e-5, e  # complex64 rounding, not the FP64 operator
+
+
+@needs_oracle
+def test_mixed_plan_keeps_the_fp64_operator(case_files, ref_ops):
+    from mlfma_pmchwt_b200 import mesh as M
+    op, ref = mixed_op(case_files, "sphere_s3_lossy"), ref_ops("sphere_s3_lossy")
+    x = M.unit_disk_vector(op.n, 0)
+    assert rel(op.apply_ax(x), ref.apply(x)) < 1e-10
+
+
+def test_refinement_reaches_fp64_tolerance(case_files):
+    from mlfma_pmchwt_b200 import plane_wave
+    op = mixed_op(case_files, "sphere_s3_lossy")
+    V = op.compute_v_pmchwt(*plane_wave(0.0, 0.0, 0.0))
+    x, st = op.solve_mixed(V, itr_max=2000, mr=50, tol_rel=1e-9, tol_abs=0.0, inner_its=8, refine_max=12)
+    assert st["converged"] and st["refinements"] >= 2
+    assert rel(op.apply_ax(x), V) < 1e-9          # the FP64 residual, recomputed
+    assert np.all(np.diff(st["history"]) < 0)     # every refinement step gains
+    xf, sf = op.matrix_solver(V, itr_max=2000, mr=50, tol_rel=1e-9, tol_abs=0.0, inner_its=8)
+    assert sf["converged"] and rel(x, xf) < 1e-7
+
+
+def test_lockstep_mixed_solve(case_files):
+    from mlfma_pmchwt_b200 import plane_wave
+    op = mixed_op(case_files, "sphere_s3_lossy")
+    B = np.stack([op.compute_v_pmchwt(*plane_wave(90.0 * (j % 2), 180.0 * j / 4, 0.0)) for j in range(5)])
+    X, st = op.solve_mixed_batch(B, itr_max=2000, mr=50, tol_rel=1e-8, tol_abs=0.0, inner_its=8, refine_max=12)
+    assert all(s["converged"] for s in st)
+    W = op.apply_batch(X)
+    for j in range(5):
+        assert rel(W[j], B[j]) < 1e-8
+
+
+def test_fp64_plan_rejects_mixed_calls(case_files):
+    from mlfma_pmchwt_b200 import MLFMM, MlfmaError
+    m, p, eps, leaf = case_files["sphere_s2"]
+    op = MLFMM(m, freq=FREQ, eps_r=eps, leaf_coeff=leaf, device=0)
+    with pytest.raises(MlfmaError):
+        op.apply_ax_mixed(np.zeros(op.n, dtype=complex))
+    with pytest.raises(MlfmaError):
+        op.solve_mixed(np.ones(op.n, dtype=complex))
