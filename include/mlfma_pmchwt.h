@@ -158,7 +158,9 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  *                  each source of the siblings' union once, every level of a
  *                  medium in one launch; 3 = warp per box, 8 Morton-consecutive
  *                  boxes per CTA sharing their source patterns through L1, every
- *                  level of a medium in one launch.
+ *                  level of a medium in one launch; 4 = warp per pair of
+ *                  Morton-consecutive boxes over their merged lists (each source
+ *                  pattern loaded once for both), every level in one launch.
  *   "up.variant"   0 = 9-tap gather per parent direction; 1 = separable
  *                  phi-then-theta interpolation in bands of theta rows (default);
  *                  2 = one thread per (parent, direction) for all 6 components.
@@ -172,7 +174,7 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  * at their current values) over `applies` applies of the plan's own operator
  * (device vectors owned by the plan) and keeps the fastest; variant_ms (may be
  * NULL) receives the per-apply ms of every value, keys in that order
- * (11 entries: m2l 0-3, up 0-2, l2l 0-1, agg 0-1). */
+ * (12 entries: m2l 0-4, up 0-2, l2l 0-1, agg 0-1). */
 MLFMA_API int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value);
 MLFMA_API int mlfma_get_tuning(const mlfma_plan* plan, const char* key);
 MLFMA_API int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms);

@@ -250,7 +250,7 @@ struct TuningKey {
   int count;  // values 0 .. count-1
 };
 constexpr TuningKey kTuningKeys[] = {
-    {"m2l.variant", &mlfma::Tuning::m2l_variant, 4},
+    {"m2l.variant", &mlfma::Tuning::m2l_variant, 5},
     {"up.variant", &mlfma::Tuning::up_variant, 3},
     {"l2l.variant", &mlfma::Tuning::l2l_variant, 2},
     {"agg.variant", &mlfma::Tuning::agg_variant, 2},

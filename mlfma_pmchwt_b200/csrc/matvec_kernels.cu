@@ -598,6 +598,72 @@ __global__ void __launch_bounds__(kThreads) l2l_kernel(L2lArg a) {
   *out = cadd(*out, acc);
 }
 
+// Translation, warp per box pair: a CTA takes 4 pairs of Morton-consecutive
+// boxes (2g, 2g+1; mostly siblings) and 32 directions. A lane walks the
+// pair's merged, source-ordered interaction lists: each source pattern is
+// loaded once and applied to whichever of the two boxes lists it, with that
+// box's transfer factor. Each box still sums its sources in ascending order.
+constexpr int kPairWarps = 4;
+
+template <class C>
+struct M2lPairSeg {
+  const C* S;
+  C* Bm;
+  const C* tfw;
+  const int* pair_ptr;
+  const int* pair_src;
+  const int2* pair_vec;
+  int B, K, nchunk, cta_begin;
+};
+template <class C>
+struct M2lPairArg {
+  M2lPairSeg<C> seg[kM2lMaxSeg];
+  int nseg;
+};
+
+template <class C>
+__global__ void __launch_bounds__(32 * kPairWarps) m2l_pair_kernel(const __grid_constant__ M2lPairArg<C> a) {
+  int si = 0;
+  while (si + 1 < a.nseg && static_cast<int>(blockIdx.x) >= a.seg[si + 1].cta_begin) ++si;
+  const M2lPairSeg<C>& g = a.seg[si];
+  const int local = blockIdx.x - g.cta_begin;
+  const int grp = local / g.nchunk;
+  const int pg = grp * kPairWarps + (threadIdx.x >> 5);
+  const int k = (local - grp * g.nchunk) * 32 + (threadIdx.x & 31);
+  const int K = g.K;
+  if (2 * pg >= g.B || k >= K) return;
+  C a0[6], a1[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) a0[c] = a1[c] = Cx<C>::zero();
+  const int e1 = g.pair_ptr[pg + 1];
+  for (int e = g.pair_ptr[pg]; e < e1; ++e) {
+    const int src = __ldg(g.pair_src + e);
+    const int2 v = __ldg(g.pair_vec + e);
+    const C* p = g.S + static_cast<size_t>(src) * 6 * K + k;
+    C sv[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) sv[c] = __ldg(p + static_cast<size_t>(c) * K);
+    if (v.x >= 0) {
+      const C t = __ldg(g.tfw + static_cast<size_t>(v.x) * K + k);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) a0[c] = cfma(t, sv[c], a0[c]);
+    }
+    if (v.y >= 0) {
+      const C t = __ldg(g.tfw + static_cast<size_t>(v.y) * K + k);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) a1[c] = cfma(t, sv[c], a1[c]);
+    }
+  }
+  C* out0 = g.Bm + static_cast<size_t>(2 * pg) * 6 * K + k;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) out0[static_cast<size_t>(c) * K] = a0[c];
+  if (2 * pg + 1 < g.B) {
+    C* out1 = g.Bm + static_cast<size_t>(2 * pg + 1) * 6 * K + k;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) out1[static_cast<size_t>(c) * K] = a1[c];
+  }
+}
+
 template <class C>
 struct L2lSepArg {
   C* Bm;                 // child level (accumulated into)
@@ -969,6 +1035,21 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
 // Translations of every level of medium m (independent of each other).
 void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
   const int L = P.maxL;
+  if (P.tuning.m2l_variant == 4) {
+    if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+    M2lPairArg<double2> a{};
+    int ctas = 0;
+    for (int l = 2; l <= L; ++l) {
+      const MediumLevel& cm = P.ml[m][l];
+      M2lPairSeg<double2>& g = a.seg[a.nseg++];
+      g = M2lPairSeg<double2>{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, P.lv[l].pair_ptr, P.lv[l].pair_src,
+                              P.lv[l].pair_vec,    P.lv[l].B,           cm.K,   (cm.K + 31) / 32,  ctas};
+      const int G = (P.lv[l].B + 1) / 2;
+      ctas += ((G + kPairWarps - 1) / kPairWarps) * g.nchunk;
+    }
+    m2l_pair_kernel<double2><<<ctas, 32 * kPairWarps, 0, s>>>(a);
+    return;
+  }
   if (P.tuning.m2l_variant == 3) {
     if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
     M2lWarpArg<double2> a{};
@@ -1054,6 +1135,29 @@ void fill_leaf_common(const Plan& P, Arg& a) {
   a.etai = Cx<C>::from(c2(P.etai.real(), P.etai.imag()));
 }
 
+// Medium 1's tree passes go to the plan's second stream, forked from and
+// joined back into s; with stage profiling on, both media stay on s so that
+// the stage events bracket one medium at a time.
+struct MediumStreams {
+  Plan& P;
+  cudaStream_t s;
+  bool two;
+  MediumStreams(Plan& P_, cudaStream_t s_, bool concurrent) : P(P_), s(s_), two(concurrent && P_.stream2) {
+    if (two) {
+      MLFMA_CUDA(cudaEventRecord(P.ev_fork, s));
+      MLFMA_CUDA(cudaStreamWaitEvent(P.stream2, P.ev_fork, 0));
+    }
+  }
+  cudaStream_t of(int m) const { return two && m == 1 ? P.stream2 : s; }
+  void join() {
+    if (two) {
+      MLFMA_CUDA(cudaEventRecord(P.ev_join, P.stream2));
+      MLFMA_CUDA(cudaStreamWaitEvent(s, P.ev_join, 0));
+      two = false;
+    }
+  }
+};
+
 cudaEvent_t* profiler_events(Plan& P, cudaStream_t s) {
   if (!P.prof.on) return nullptr;
   if (P.prof.used == P.prof.sets.size()) {
@@ -1109,16 +1213,19 @@ template <class C>
 void apply_fixed(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   const int L = P.maxL;
   LeafArg<C> a{};
+  MediumStreams ms(P, s, true);
   for (int m = 0; m < 2; ++m) {
+    const cudaStream_t sm = ms.of(m);
     const MediumLevel& leaf = P.ml[m][L];
-    agg_kernel<C><<<dim3(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+    agg_kernel<C><<<dim3(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads), kThreads, 0, sm>>>(
         Store<C>::Vs(P, m), P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, Store<C>::S(leaf));
-    tree_pass_fixed<C>(P, m, Store<C>::S(leaf), Store<C>::Bm(leaf), s);
+    tree_pass_fixed<C>(P, m, Store<C>::S(leaf), Store<C>::Bm(leaf), sm);
     a.Vf[m] = Store<C>::Vf(P, m);
     a.Bm[m] = Store<C>::Bm(leaf);
     a.khat[m] = leaf.khat;
     a.K[m] = leaf.K;
   }
+  ms.join();
   fill_leaf_common(P, a);
   a.x = x;
   a.w = w;
@@ -1147,8 +1254,12 @@ void apply_batch_fixed(Plan& P, int R, const double2* X, long long ldx, double2*
     ag.N = P.N;
     ag.R = rn;
     agg_batch_kernel<C, kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
-    for (int j = 0; j < rn; ++j)
-      for (int m = 0; m < 2; ++m) tree_pass_fixed<C>(P, m, Store<C>::bS(P, m, j), Store<C>::bB(P, m, j), s);
+    {
+      MediumStreams ms(P, s, true);
+      for (int j = 0; j < rn; ++j)
+        for (int m = 0; m < 2; ++m) tree_pass_fixed<C>(P, m, Store<C>::bS(P, m, j), Store<C>::bB(P, m, j), ms.of(m));
+      ms.join();
+    }
     LeafBatchArg<C> lb{};
     for (int m = 0; m < 2; ++m) {
       lb.Vf[m] = Store<C>::Vf(P, m);
@@ -1187,21 +1298,24 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
     a.N = P.N;
     agg_box_kernel<<<dim3(P.lv[L].B, 2), kThreads, 0, s>>>(a);
   }
+  MediumStreams ms(P, s, ev == nullptr);
   for (int m = 0; m < 2; ++m) {
+    const cudaStream_t sm = ms.of(m);
     const MediumLevel& leaf = P.ml[m][L];
     if (P.tuning.agg_variant == 0) {
       dim3 g(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads);
-      agg_kernel<double2><<<g, kThreads, 0, s>>>(P.d_Vs[m], P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, leaf.S);
+      agg_kernel<double2><<<g, kThreads, 0, sm>>>(P.d_Vs[m], P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, leaf.S);
     }
     if (ev) MLFMA_CUDA(cudaEventRecord(ev[1 + 4 * m], s));
     const LeafView v{leaf.S, leaf.Bm};
-    launch_up(P, m, v, s);
+    launch_up(P, m, v, sm);
     if (ev) MLFMA_CUDA(cudaEventRecord(ev[2 + 4 * m], s));
-    launch_m2l(P, m, v, s);
+    launch_m2l(P, m, v, sm);
     if (ev) MLFMA_CUDA(cudaEventRecord(ev[3 + 4 * m], s));
-    launch_l2l(P, m, v, s);
+    launch_l2l(P, m, v, sm);
     if (ev) MLFMA_CUDA(cudaEventRecord(ev[4 + 4 * m], s));
   }
+  ms.join();
   LeafArg<double2> a{};
   for (int m = 0; m < 2; ++m) {
     a.Vf[m] = P.d_Vf[m];
@@ -1254,13 +1368,17 @@ void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2
     ag.N = P.N;
     ag.R = rn;
     agg_batch_kernel<double2, kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
-    for (int j = 0; j < rn; ++j)
-      for (int m = 0; m < 2; ++m) {
-        const LeafView v{P.bS[m][j], P.bB[m][j]};
-        launch_up(P, m, v, s);
-        launch_m2l(P, m, v, s);
-        launch_l2l(P, m, v, s);
-      }
+    {
+      MediumStreams ms(P, s, true);
+      for (int j = 0; j < rn; ++j)
+        for (int m = 0; m < 2; ++m) {
+          const LeafView v{P.bS[m][j], P.bB[m][j]};
+          launch_up(P, m, v, ms.of(m));
+          launch_m2l(P, m, v, ms.of(m));
+          launch_l2l(P, m, v, ms.of(m));
+        }
+      ms.join();
+    }
     LeafBatchArg<double2> lb{};
     for (int m = 0; m < 2; ++m) {
       lb.Vf[m] = P.d_Vf[m];

@@ -1,6 +1,7 @@
 // Plan construction: host tables, device upload, device setup kernels.
 #include <algorithm>
 #include <chrono>
+#include <cstdint>
 #include <cmath>
 #include <cstdio>
 #include <map>
@@ -22,6 +23,12 @@ Plan::~Plan() {
       for (cudaEvent_t e : set) cudaEventDestroy(e);
     for (void* p : allocations) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
+    if (stream2) {
+      cudaStreamSynchronize(stream2);
+      cudaStreamDestroy(stream2);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 }
 
@@ -131,6 +138,9 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   // ------------------------------------------------------------- device
   MLFMA_CUDA(cudaSetDevice(prm.device));
   MLFMA_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+  MLFMA_CUDA(cudaStreamCreateWithFlags(&P->stream2, cudaStreamNonBlocking));
+  MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
+  MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
   cudaStream_t s = P->stream;
   const Mesh& Me = P->mesh;
   const Rwg& R = P->rwg;
@@ -341,6 +351,29 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
           std::vector<int> fv(T.lv[l].far_off.size());
           for (size_t e = 0; e < fv.size(); ++e) fv[e] = off2vec[T.lv[l].far_off[e]];
           P->lv[l].far_vec = P->upload(fv);
+          // merged lists of box pairs (2g, 2g+1)
+          const Level& Lv = T.lv[l];
+          const int B = Lv.size(), G = (B + 1) / 2;
+          std::vector<int> pptr(G + 1, 0), psrc;
+          std::vector<int2> pvec;
+          for (int g = 0; g < G; ++g) {
+            const int b0 = 2 * g, b1 = std::min(2 * g + 1, B - 1);
+            int e0 = Lv.far_ptr[b0], e1 = b1 != b0 ? Lv.far_ptr[b1] : 0;
+            const int f0 = Lv.far_ptr[b0 + 1], f1 = b1 != b0 ? Lv.far_ptr[b1 + 1] : 0;
+            while (e0 < f0 || e1 < f1) {
+              const int s0 = e0 < f0 ? Lv.far_idx[e0] : INT32_MAX, s1 = e1 < f1 ? Lv.far_idx[e1] : INT32_MAX;
+              const int src = std::min(s0, s1);
+              int2 v = make_int2(-1, -1);
+              if (s0 == src) v.x = fv[e0++];
+              if (s1 == src) v.y = fv[e1++];
+              psrc.push_back(src);
+              pvec.push_back(v);
+            }
+            pptr[g + 1] = static_cast<int>(psrc.size());
+          }
+          P->lv[l].pair_ptr = P->upload(pptr);
+          P->lv[l].pair_src = P->upload(psrc);
+          P->lv[l].pair_vec = P->upload(pvec);
         }
         std::vector<double> rhat;
         std::vector<int> hoff, hL;

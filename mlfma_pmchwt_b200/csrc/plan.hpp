@@ -77,6 +77,11 @@ struct DevLevel {
   int* far_idx = nullptr;
   int* far_off = nullptr;
   int* far_vec = nullptr;      // transfer-factor row of each interaction-list entry
+  // boxes in pairs (2g, 2g+1): the merged, source-ordered interaction lists of
+  // each pair with the transfer-factor row of either member (-1: not in its list)
+  int* pair_ptr = nullptr;     // [ceil(B/2) + 1]
+  int* pair_src = nullptr;
+  int2* pair_vec = nullptr;
   long long far_pairs = 0;
   int* coord = nullptr;        // [3 * B] integer box coordinates
   int* usrc_ptr = nullptr;     // per parent box (level - 1): union of its children's
@@ -94,7 +99,8 @@ struct DevLevel {
 struct Tuning {
   int m2l_variant = 2;         // 0: one thread per (box, direction); 1: sibling-group tiles;
                                // 2: octant registers over the sibling union, all levels per launch;
-                               // 3: warp per box, 8 Morton-consecutive boxes per CTA, all levels per launch
+                               // 3: warp per box, 8 Morton-consecutive boxes per CTA, all levels per launch;
+                               // 4: warp per box pair (merged lists), 8 pairs per CTA, all levels per launch
   int l2l_variant = 1;         // 0: 2-D transposed taps per child direction; 1: separable
   int up_variant = 1;          // 0: 9-tap gather per parent direction; 1: separable in bands;
                                // 2: 9-tap gather, all 6 components per thread
@@ -173,6 +179,10 @@ struct Plan {
   double2* d_wb = nullptr;
   int xb_cap = 0;
   cudaStream_t stream = nullptr;
+  // the second medium's tree passes run on stream2, forked from and joined
+  // back into the caller's stream with these events
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   StageProfiler prof;
   size_t bytes = 0;
   std::vector<void*> allocations;
