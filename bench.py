@@ -41,10 +41,10 @@ def launches_per_apply(max_level: int, tune: dict) -> int:
     """Kernels one operator apply launches: the aggregation (one launch for
     both media with agg variant 1, else one per medium); per medium one
     interpolation per level pair, the translations (one launch for every
-    level with m2l variants 2-4, else one per level) and one anterpolation per
+    level with m2l variants 2-5, else one per level) and one anterpolation per
     level pair; then the leaf testing + near-field kernel."""
     lv = max_level - 2
-    m2l = 1 if tune["m2l.variant"] in (2, 3, 4) else lv + 1
+    m2l = 1 if tune["m2l.variant"] in (2, 3, 4, 5) else lv + 1
     agg = 1 if tune.get("agg.variant", 0) == 1 else 2
     return agg + 2 * (lv + m2l + lv) + 1
 
@@ -201,11 +201,11 @@ def cpu_baseline_reference(args, wl, rank: int) -> dict | None:
 
 
 def run_reference_arm(args):
-    world, rank, local = dist_setup()
-    if rank != 0:
+    # the reference's CPU matvec runs on rank 0 alone; no collective is needed
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
     wl = workload(args)
-    base = cpu_baseline_reference(args, wl, rank)
+    base = cpu_baseline_reference(args, wl, 0)
     if base is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmlfma_ref.so not built"}))
         return 0
@@ -218,6 +218,23 @@ def run_reference_arm(args):
             "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def measured_traffic(workload: str, stage: str, tune: dict):
+    """DRAM bytes (read + write) per apply of a stage's kernels, from the
+    one-pass ncu capture recorded in profiles/dram_traffic.json (command
+    there), when it was taken on this workload with the same kernel choice;
+    else None."""
+    f = ROOT / "profiles" / "dram_traffic.json"
+    if not f.exists():
+        return None
+    rec = json.loads(f.read_text())
+    if rec.get("workload") != workload:
+        return None
+    ent = rec.get("stages", {}).get(stage)
+    if not ent or any(tune.get(k) != v for k, v in ent.get("tuning", {}).items()):
+        return None
+    return ent["dram_bytes_per_apply"]
 
 
 def parse_tuning(spec: str) -> dict | None:
@@ -286,6 +303,35 @@ def multi_rhs_study(args, local: int) -> dict:
         "fp64_1e-3_max": round(float(dd.max()), 5), "fp64_1e-3_median": round(float(np.median(dd)), 5)}
     op.close()
     return out
+
+
+def bodies_study(args, local: int) -> dict:
+    """24 uneven dielectric bodies (mesh.uneven_bodies(1): icospheres,
+    ellipsoids, superellipsoids; 3,840-61,440 unknowns; lossy eps_r), 16
+    plane waves each (theta_i = i * 180/15, phi = 0, polarisation alternating),
+    solved to 1e-3 per body by lockstep FGMRES with the complex64 operator
+    inside FP64 refinement. Bodies go one after another, each with its own
+    plan; transfer factors with the complex argument (the bodies are lossy)."""
+    from mlfma_pmchwt_b200 import MLFMM, plane_wave
+    from mlfma_pmchwt_b200 import mesh as M
+    rows, t_all = [], time.perf_counter()
+    for b in M.uneven_bodies(1, FREQ):
+        t0 = time.perf_counter()
+        op = MLFMM(b["mesh"], freq=FREQ, eps_r=b["eps_r"], leaf_coeff=0.25, device=local, precision="mixed",
+                   tf_complex_argument=True)
+        setup = time.perf_counter() - t0
+        B = np.stack([op.compute_v_pmchwt(*plane_wave(90.0 * (i % 2), 12.0 * i, 0.0)) for i in range(16)])
+        t1 = time.perf_counter()
+        X, st = op.solve_mixed_batch(B, itr_max=600, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.inner_its)
+        solve = time.perf_counter() - t1
+        rows.append({"kind": b["kind"], "unknowns": op.n, "eps_r": [round(b["eps_r"].real, 3), round(b["eps_r"].imag, 4)],
+                     "setup_s": round(setup, 3), "solve_s": round(solve, 3), "converged": sum(s_["converged"] for s_ in st),
+                     "iterations_mean": round(float(np.mean([s_["iterations"] for s_ in st])), 1)})
+        op.close()
+    total = time.perf_counter() - t_all
+    return {"bodies": len(rows), "rhs": 16 * len(rows), "total_s": round(total, 2),
+            "s_per_rhs": round(total / (16 * len(rows)), 4),
+            "converged": sum(r["converged"] for r in rows), "per_body": rows}
 
 
 def run_product(args):
@@ -378,8 +424,9 @@ def run_product(args):
     per_apply_ms = {k: v / max(napp, 1) for k, v in stage_ms.items()}
     dom = max(per_apply_ms, key=per_apply_ms.get)
     achieved = sb[dom] / (per_apply_ms[dom] / 1000.0) / 1e9
+    traffic = measured_traffic(wl["name"], dom, tune)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": None,
+                "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": traffic,
                 "algorithmic_bytes": sb[dom],
                 "stage_ms_per_apply": {k: round(v, 4) for k, v in per_apply_ms.items()},
                 "stage_note": "stage times from a pass with the two media one after the other; "
@@ -456,6 +503,8 @@ def run_product(args):
         line["mixed_precision"] = mixed
     if args.rhs > 0 and world == 1:
         line["multi_rhs"] = multi_rhs_study(args, local)
+    if args.bodies and world == 1:
+        line["uneven_bodies"] = bodies_study(args, local)
     if solve:
         line["solve"] = solve
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -489,6 +538,7 @@ def main(argv=None):
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference matvecs to time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rhs", type=int, default=128, help="incidences of the multi-RHS study (0: skip)")
+    ap.add_argument("--bodies", action="store_true", help="also run the 24-body uneven batch study")
     ap.add_argument("--no-mixed", dest="mixed", action="store_false",
                     help="skip the complex64 (mixed-precision) operator and solve")
     ap.add_argument("--tuning", default="auto",

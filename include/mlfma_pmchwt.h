@@ -160,10 +160,13 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  *                  boxes per CTA sharing their source patterns through L1, every
  *                  level of a medium in one launch; 4 = warp per pair of
  *                  Morton-consecutive boxes over their merged lists (each source
- *                  pattern loaded once for both), every level in one launch.
+ *                  pattern loaded once for both), every level in one launch;
+ *                  5 = the same with J and M halves on separate warps.
  *   "up.variant"   0 = 9-tap gather per parent direction; 1 = separable
  *                  phi-then-theta interpolation in bands of theta rows (default);
- *                  2 = one thread per (parent, direction) for all 6 components.
+ *                  2 = one thread per (parent, direction) for all 6 components;
+ *                  3 = separable in registers: a thread takes a phi column of a
+ *                  band of 4 parent theta rows.
  *   "l2l.variant"  0 = transposed 9-tap gather per child direction;
  *                  1 = separable transposed theta-then-phi (default).
  *   "agg.variant"  0 = one thread per (leaf box, direction), one launch per
@@ -174,7 +177,7 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  * at their current values) over `applies` applies of the plan's own operator
  * (device vectors owned by the plan) and keeps the fastest; variant_ms (may be
  * NULL) receives the per-apply ms of every value, keys in that order
- * (12 entries: m2l 0-4, up 0-2, l2l 0-1, agg 0-1). */
+ * (14 entries: m2l 0-5, up 0-3, l2l 0-1, agg 0-1). */
 MLFMA_API int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value);
 MLFMA_API int mlfma_get_tuning(const mlfma_plan* plan, const char* key);
 MLFMA_API int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms);

@@ -250,8 +250,8 @@ struct TuningKey {
   int count;  // values 0 .. count-1
 };
 constexpr TuningKey kTuningKeys[] = {
-    {"m2l.variant", &mlfma::Tuning::m2l_variant, 5},
-    {"up.variant", &mlfma::Tuning::up_variant, 3},
+    {"m2l.variant", &mlfma::Tuning::m2l_variant, 6},
+    {"up.variant", &mlfma::Tuning::up_variant, 4},
     {"l2l.variant", &mlfma::Tuning::l2l_variant, 2},
     {"agg.variant", &mlfma::Tuning::agg_variant, 2},
 };

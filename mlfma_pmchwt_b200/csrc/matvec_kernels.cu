@@ -208,6 +208,95 @@ __global__ void __launch_bounds__(kThreads) up6_kernel(UpArg<double2> a) {
   for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * a.Kp] = acc[c];
 }
 
+// Interpolation (m2m), separable in registers: thread per (parent box, band
+// of kUpColBand parent theta rows, component, parent phi column). For each
+// child it interpolates in phi each child theta row the band needs (3 taps;
+// kept in the thread's own shared-memory slots, so no barrier), then forms
+// the band's parent directions from 3 theta taps each, times the child's
+// shift phase, accumulated over the children. About 5.5 loads per output
+// against 10 for the 9-tap gather.
+template <class C>
+struct UpColArg {
+  const C* Sc;
+  C* Sp;
+  const int* child_begin;
+  const int* octant;
+  const int* pidx;
+  const double* lp;
+  const double* lt;
+  const int* row_ptr;  // per band: the child theta rows it needs
+  const int* row;
+  const int* tpos;     // [nthp][3]: band row of each theta tap
+  const C* ph_up;
+  int nthp, nphp, nphc, Kc;
+};
+
+template <class C>
+__global__ void __launch_bounds__(kThreads) up_col_kernel(UpColArg<C> a) {
+  using R = typename Cx<C>::real;
+  __shared__ C rv[kUpColRows][kThreads];
+  const int P = blockIdx.x, bi = blockIdx.y;
+  const int q = blockIdx.z * blockDim.x + threadIdx.x;
+  if (q >= 6 * a.nphp) return;
+  const int c = q / a.nphp, p = q - c * a.nphp;
+  const int t0 = bi * kUpColBand, nt = min(kUpColBand, a.nthp - t0);
+  const int r0 = a.row_ptr[bi], nr = a.row_ptr[bi + 1] - r0;
+  int pj[3];
+  R wp[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    pj[j] = __ldg(a.pidx + 3 * p + j);
+    wp[j] = static_cast<R>(__ldg(a.lp + 3 * p + j));
+  }
+  int tp[kUpColBand][3];
+  R wt[kUpColBand][3];
+#pragma unroll
+  for (int t = 0; t < kUpColBand; ++t)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const bool in = t < nt;
+      tp[t][i] = in ? __ldg(a.tpos + 3 * (t0 + t) + i) : 0;
+      wt[t][i] = in ? static_cast<R>(__ldg(a.lt + 3 * (t0 + t) + i)) : R(0);
+    }
+  int rowoff[kUpColRows];
+#pragma unroll
+  for (int r = 0; r < kUpColRows; ++r) rowoff[r] = r < nr ? __ldg(a.row + r0 + r) * a.nphc : 0;
+  C acc[kUpColBand];
+#pragma unroll
+  for (int t = 0; t < kUpColBand; ++t) acc[t] = Cx<C>::zero();
+  const int Kp = a.nthp * a.nphp;
+  C(*mine)[kThreads] = rv;
+  const int me = threadIdx.x;
+  const int c1 = a.child_begin[P + 1];
+  for (int ch = a.child_begin[P]; ch < c1; ++ch) {
+    const C* sc = a.Sc + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
+#pragma unroll
+    for (int r = 0; r < kUpColRows; ++r) {
+      if (r < nr) {
+        const C* srow = sc + rowoff[r];
+        C v = cscale(__ldg(srow + pj[0]), wp[0]);
+        v = cfmas(wp[1], __ldg(srow + pj[1]), v);
+        v = cfmas(wp[2], __ldg(srow + pj[2]), v);
+        mine[r][me] = v;
+      }
+    }
+    const C* ph = a.ph_up + a.octant[ch] * Kp + t0 * a.nphp + p;
+#pragma unroll
+    for (int t = 0; t < kUpColBand; ++t) {
+      if (t < nt) {
+        C v = cscale(mine[tp[t][0]][me], wt[t][0]);
+        v = cfmas(wt[t][1], mine[tp[t][1]][me], v);
+        v = cfmas(wt[t][2], mine[tp[t][2]][me], v);
+        acc[t] = cfma(__ldg(ph + t * a.nphp), v, acc[t]);
+      }
+    }
+  }
+  C* out = a.Sp + (static_cast<size_t>(P) * 6 + c) * Kp + t0 * a.nphp + p;
+#pragma unroll
+  for (int t = 0; t < kUpColBand; ++t)
+    if (t < nt) out[t * a.nphp] = acc[t];
+}
+
 struct UpSepArg {
   const double2* Sc;   // child level patterns [Bc][6][Kc]
   double2* Sp;         // parent level patterns [Bp][6][Kp]
@@ -664,6 +753,54 @@ __global__ void __launch_bounds__(32 * kPairWarps) m2l_pair_kernel(const __grid_
   }
 }
 
+// The same walk with each pair's J and M halves on two warps: a CTA of 8
+// warps takes 4 pairs x {J, M}; a lane keeps 3 components of both boxes
+// (half the registers of m2l_pair_kernel, twice the resident warps), and
+// the transfer factors the two halves both load come from L1.
+template <class C>
+__global__ void __launch_bounds__(64 * kPairWarps) m2l_pairh_kernel(const __grid_constant__ M2lPairArg<C> a) {
+  int si = 0;
+  while (si + 1 < a.nseg && static_cast<int>(blockIdx.x) >= a.seg[si + 1].cta_begin) ++si;
+  const M2lPairSeg<C>& g = a.seg[si];
+  const int local = blockIdx.x - g.cta_begin;
+  const int grp = local / g.nchunk;
+  const int w = threadIdx.x >> 5;
+  const int pg = grp * kPairWarps + (w >> 1), h = w & 1;
+  const int k = (local - grp * g.nchunk) * 32 + (threadIdx.x & 31);
+  const int K = g.K;
+  if (2 * pg >= g.B || k >= K) return;
+  C a0[3], a1[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) a0[c] = a1[c] = Cx<C>::zero();
+  const int e1 = g.pair_ptr[pg + 1];
+  for (int e = g.pair_ptr[pg]; e < e1; ++e) {
+    const int src = __ldg(g.pair_src + e);
+    const int2 v = __ldg(g.pair_vec + e);
+    const C* p = g.S + (static_cast<size_t>(src) * 6 + 3 * h) * K + k;
+    C sv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sv[c] = __ldg(p + static_cast<size_t>(c) * K);
+    if (v.x >= 0) {
+      const C t = __ldg(g.tfw + static_cast<size_t>(v.x) * K + k);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) a0[c] = cfma(t, sv[c], a0[c]);
+    }
+    if (v.y >= 0) {
+      const C t = __ldg(g.tfw + static_cast<size_t>(v.y) * K + k);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) a1[c] = cfma(t, sv[c], a1[c]);
+    }
+  }
+  C* out0 = g.Bm + (static_cast<size_t>(2 * pg) * 6 + 3 * h) * K + k;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out0[static_cast<size_t>(c) * K] = a0[c];
+  if (2 * pg + 1 < g.B) {
+    C* out1 = g.Bm + (static_cast<size_t>(2 * pg + 1) * 6 + 3 * h) * K + k;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out1[static_cast<size_t>(c) * K] = a1[c];
+  }
+}
+
 template <class C>
 struct L2lSepArg {
   C* Bm;                 // child level (accumulated into)
@@ -687,8 +824,16 @@ __host__ __device__ __forceinline__ int l2l_band_rows(int ntc, int npp) {
   return max(1, min(ntc, kL2lBand / (6 * npp)));
 }
 
-// Anterpolation (l2l), separable: one CTA per (child box, band of child theta
-// rows) does all 6 components. The parent's incoming pattern is shifted to the child centre
+// CTAs per child box: one per band on levels with few boxes (so that the
+// level fills the GPU), else one CTA walks all the bands of its box.
+constexpr int kL2lSplitBoxes = 1024;
+inline int l2l_grid_y(int boxes, int ntc, int npp) {
+  const int nband = (ntc + l2l_band_rows(ntc, npp) - 1) / l2l_band_rows(ntc, npp);
+  return boxes < kL2lSplitBoxes ? nband : 1;
+}
+
+// Anterpolation (l2l), separable: a CTA per child box (and, on levels with few
+// boxes, per band of child theta rows) does all 6 components. The parent's incoming pattern is shifted to the child centre
 // and spread onto the child grid by the transposed theta interpolation (into
 // a shared-memory band of child rows x parent phi columns x 6 components),
 // then by the transposed phi interpolation, and added to the child's Bm. The
@@ -704,10 +849,10 @@ __global__ void __launch_bounds__(256) l2l_sep_kernel(L2lSepArg<C> a) {
   const C* ph = a.ph_dn + a.octant[b] * Kp;
   const C* bp = a.Bp + static_cast<size_t>(a.parent[b]) * 6 * Kp;
   C* out = a.Bm + static_cast<size_t>(b) * 6 * Kc;
-  {
-    const int tc0 = blockIdx.y * band_rows;  // one band of child theta rows per CTA
+  for (int tc0 = blockIdx.y * band_rows; tc0 < a.ntc; tc0 += gridDim.y * band_rows) {
     const int rows = min(band_rows, a.ntc - tc0);
     const int stride = rows * a.npp;
+    __syncthreads();
     for (int e = threadIdx.x; e < stride; e += blockDim.x) {
       const int r = e / a.npp, pp = e - r * a.npp;
       const int tc = tc0 + r;
@@ -1013,7 +1158,13 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
     const MediumLevel& pm = P.ml[m][l];
     const MediumLevel& cm = P.ml[m][l + 1];
     const double2* Sc = level_S(P, m, l + 1, v);
-    if (P.tuning.up_variant == 2) {
+    if (P.tuning.up_variant == 3 && pm.up4_row_ptr) {
+      UpColArg<double2> a{Sc,     pm.S,           P.lv[l].child_begin, P.lv[l + 1].octant, pm.pidx, pm.lp,
+                          pm.lt,  pm.up4_row_ptr, pm.up4_row,          pm.up4_tpos,        pm.ph_up, pm.nth,
+                          pm.nph, cm.nph,         cm.K};
+      up_col_kernel<double2>
+          <<<dim3(P.lv[l].B, pm.up4_nband, (6 * pm.nph + kThreads - 1) / kThreads), kThreads, 0, s>>>(a);
+    } else if (P.tuning.up_variant == 2) {
       UpArg<double2> a{Sc, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
                        pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
       up6_kernel<<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads), kThreads, 0, s>>>(a);
@@ -1035,7 +1186,7 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
 // Translations of every level of medium m (independent of each other).
 void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
   const int L = P.maxL;
-  if (P.tuning.m2l_variant == 4) {
+  if (P.tuning.m2l_variant == 4 || P.tuning.m2l_variant == 5) {
     if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
     M2lPairArg<double2> a{};
     int ctas = 0;
@@ -1047,7 +1198,10 @@ void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
       const int G = (P.lv[l].B + 1) / 2;
       ctas += ((G + kPairWarps - 1) / kPairWarps) * g.nchunk;
     }
-    m2l_pair_kernel<double2><<<ctas, 32 * kPairWarps, 0, s>>>(a);
+    if (P.tuning.m2l_variant == 5)
+      m2l_pairh_kernel<double2><<<ctas, 64 * kPairWarps, 0, s>>>(a);
+    else
+      m2l_pair_kernel<double2><<<ctas, 32 * kPairWarps, 0, s>>>(a);
     return;
   }
   if (P.tuning.m2l_variant == 3) {
@@ -1107,8 +1261,7 @@ void launch_l2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
       L2lSepArg<double2> b{Bc,         pm.Bm,    P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.thT_ptr,
                   cm.thT_src, cm.thT_w, cm.phT_ptr,     cm.phT_src,     cm.phT_w, cm.nth,
                   cm.nph,     pm.nth,   pm.nph};
-      const int nband = (cm.nth + l2l_band_rows(cm.nth, pm.nph) - 1) / l2l_band_rows(cm.nth, pm.nph);
-      l2l_sep_kernel<double2><<<dim3(P.lv[l].B, nband), 256, 0, s>>>(b);
+      l2l_sep_kernel<double2><<<dim3(P.lv[l].B, l2l_grid_y(P.lv[l].B, cm.nth, pm.nph)), 256, 0, s>>>(b);
     } else {
       L2lArg b{Bc, pm.Bm, P.lv[l].parent, P.lv[l].octant, pm.ph_dn, cm.tr_ptr, cm.tr_kp, cm.tr_w, cm.K, pm.K};
       dim3 gl(P.lv[l].B, (cm.K + kThreads - 1) / kThreads, 6);
@@ -1204,8 +1357,7 @@ void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s) {
     L2lSepArg<C> b{B_at(l),    B_at(l - 1), P.lv[l].parent, P.lv[l].octant, Store<C>::ph_dn(pm), cm.thT_ptr,
                    cm.thT_src, cm.thT_w,    cm.phT_ptr,     cm.phT_src,     cm.phT_w,            cm.nth,
                    cm.nph,     pm.nth,      pm.nph};
-    const int nband = (cm.nth + l2l_band_rows(cm.nth, pm.nph) - 1) / l2l_band_rows(cm.nth, pm.nph);
-    l2l_sep_kernel<C><<<dim3(P.lv[l].B, nband), 256, 0, s>>>(b);
+    l2l_sep_kernel<C><<<dim3(P.lv[l].B, l2l_grid_y(P.lv[l].B, cm.nth, pm.nph)), 256, 0, s>>>(b);
   }
 }
 

@@ -282,6 +282,23 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
           M.up_row = P->upload(rlist);
           M.up_tpos = P->upload(tpos);
         }
+        // bands of kUpColBand parent rows for the register-separable kernel
+        if (worst_band(kUpColBand) <= kUpColRows) {
+          M.up4_nband = (M.nth + kUpColBand - 1) / kUpColBand;
+          std::vector<int> rptr(M.up4_nband + 1, 0), rlist, tpos(3 * static_cast<size_t>(M.nth));
+          for (int bi = 0; bi < M.up4_nband; ++bi) {
+            band_rows(bi * kUpColBand, kUpColBand);
+            for (int t = bi * kUpColBand; t < std::min(M.nth, (bi + 1) * kUpColBand); ++t)
+              for (int i = 0; i < 3; ++i)
+                tpos[3 * t + i] =
+                    static_cast<int>(std::lower_bound(rows.begin(), rows.end(), I.tidx[3 * t + i]) - rows.begin());
+            rlist.insert(rlist.end(), rows.begin(), rows.end());
+            rptr[bi + 1] = static_cast<int>(rlist.size());
+          }
+          M.up4_row_ptr = P->upload(rptr);
+          M.up4_row = P->upload(rlist);
+          M.up4_tpos = P->upload(tpos);
+        }
       }
       if (l > 2) {
         // transposed interpolation: child direction <- (parent direction, weight)

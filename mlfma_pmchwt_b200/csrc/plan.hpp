@@ -24,6 +24,10 @@ namespace mlfma {
 // 256-thread CTA) and the staged child-row entries a band may hold (40 KiB).
 constexpr int kUpBandOut = 1024;
 constexpr int kUpBandEntries = 2560;
+// Register-separable interpolation: parent theta rows per band, and the most
+// child rows a band may need.
+constexpr int kUpColBand = 4;
+constexpr int kUpColRows = 8;
 
 struct MediumLevel {
   int L = 0, nth = 0, nph = 0, K = 0;
@@ -49,6 +53,12 @@ struct MediumLevel {
   int* up_row_ptr = nullptr;
   int* up_row = nullptr;
   int* up_tpos = nullptr;
+  // the same for bands of kUpColBand rows (register-separable interpolation);
+  // up4_row_ptr is null when a band would need more than kUpColRows child rows
+  int up4_nband = 0;
+  int* up4_row_ptr = nullptr;
+  int* up4_row = nullptr;
+  int* up4_tpos = nullptr;
   // this level as child of level-1: for each child direction, the parent
   // directions that interpolate onto it and the Lagrange weight
   int* tr_ptr = nullptr;       // [K+1]
@@ -100,10 +110,12 @@ struct Tuning {
   int m2l_variant = 2;         // 0: one thread per (box, direction); 1: sibling-group tiles;
                                // 2: octant registers over the sibling union, all levels per launch;
                                // 3: warp per box, 8 Morton-consecutive boxes per CTA, all levels per launch;
-                               // 4: warp per box pair (merged lists), 8 pairs per CTA, all levels per launch
+                               // 4: warp per box pair (merged lists), 4 pairs per CTA, all levels per launch;
+                               // 5: as 4 with the J and M halves on separate warps
   int l2l_variant = 1;         // 0: 2-D transposed taps per child direction; 1: separable
   int up_variant = 1;          // 0: 9-tap gather per parent direction; 1: separable in bands;
-                               // 2: 9-tap gather, all 6 components per thread
+                               // 2: 9-tap gather, all 6 components per thread;
+                               // 3: separable in registers, 4-row bands per thread
   int agg_variant = 1;         // 0: thread per (box, direction); 1: CTA per (box, medium) streaming
                                //    the box's contiguous pattern block
 };

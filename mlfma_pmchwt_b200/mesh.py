@@ -214,3 +214,49 @@ class _MT19937_64:
                 xa ^= 0xB5026F5AA96619E9
             mt[i] = mt[(i + 156) % 312] ^ xa
         self.i = 0
+
+
+def uneven_bodies(seed: int = 1, freq_hz: float = 3.0e8) -> list[dict]:
+    """24 dielectric bodies drawn from std::mt19937_64(seed), in this order and
+    with these distributions (u = (g() >> 11) 2^-53 uniform on [0, 1)):
+      8 icospheres:      sub = 3 + floor(3u), radius = (1 + 1.5u) lambda;
+      8 ellipsoids:      semi-axes (0.5 + 2.5u) lambda each, sub = 4 + floor(2u);
+      8 superellipsoids: exponent 4, semi-axes (0.5 + 1.0u) lambda each, the
+                         subdivision (3..5) whose mean edge is closest to 0.1 lambda;
+    then for every body eps_r' = 1.5 + 4.5u and tan(delta) = 0.05u, eps_r =
+    eps_r' (1 - j tan(delta)). Returns dicts with the mesh and the material."""
+    g = _MT19937_64(seed)
+    u = lambda: (g.next() >> 11) * 2.0 ** -53
+    lam = wavelength(freq_hz)
+    bodies = []
+    for _ in range(8):
+        sub = 3 + int(3 * u())
+        r = (1.0 + 1.5 * u()) * lam
+        bodies.append(dict(kind="icosphere", mesh=icosphere(sub, r), params=dict(sub=sub, radius=r)))
+    for _ in range(8):
+        a, b, c = ((0.5 + 2.5 * u()) * lam for _ in range(3))
+        sub = 4 + int(2 * u())
+        bodies.append(dict(kind="ellipsoid", mesh=ellipsoid(sub, a, b, c), params=dict(sub=sub, axes=(a, b, c))))
+    for _ in range(8):
+        a, b, c = ((0.5 + 1.0 * u()) * lam for _ in range(3))
+        best = None
+        for sub in (3, 4, 5):
+            m = superellipsoid(sub, a, b, c, 4.0)
+            edge = _mean_edge(m)
+            if best is None or abs(edge - 0.1 * lam) < abs(best[1] - 0.1 * lam):
+                best = (m, edge, sub)
+        bodies.append(dict(kind="superellipsoid", mesh=best[0], params=dict(sub=best[2], axes=(a, b, c), power=4.0,
+                                                                           mean_edge=best[1])))
+    for b in bodies:
+        er = 1.5 + 4.5 * u()
+        td = 0.05 * u()
+        b["eps_r"] = complex(er, -er * td)
+    return bodies
+
+
+def _mean_edge(m: Mesh) -> float:
+    p = np.asarray(m.points)
+    idx = {int(i): k for k, i in enumerate(m.point_ids)}
+    fv = np.array([[idx[int(v)] for v in tri] for tri in m.face_point_ids()])
+    e = np.concatenate([np.linalg.norm(p[fv[:, i]] - p[fv[:, (i + 1) % 3]], axis=1) for i in range(3)])
+    return float(e.mean())

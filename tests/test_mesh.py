@@ -50,3 +50,21 @@ def test_unit_disk_vector():
     assert np.all(np.abs(x) <= 1.0)
     assert abs(np.mean(np.abs(x) ** 2) - 0.5) < 0.03
     np.testing.assert_array_equal(x, M.unit_disk_vector(2000, 0))
+
+
+def test_uneven_body_set():
+    """The 24-body set: order, kinds, sizes 3,840-61,440 unknowns, lossy
+    materials in range, and the first body's draws pinned."""
+    bodies = M.uneven_bodies(1)
+    assert [b["kind"] for b in bodies] == ["icosphere"] * 8 + ["ellipsoid"] * 8 + ["superellipsoid"] * 8
+    n = [3 * len(b["mesh"].face_ids) for b in bodies]  # 2N = 3 F for a closed surface
+    assert min(n) == 3840 and max(n) == 61440
+    for b in bodies:
+        e = b["eps_r"]
+        assert 1.5 <= e.real <= 6.0 and -0.05 * e.real <= e.imag <= 0.0
+    first = bodies[0]
+    assert first["params"]["sub"] == 3
+    assert abs(first["eps_r"] - complex(4.041, -0.0981)) < 1e-3
+    again = M.uneven_bodies(1)
+    for a, b in zip(bodies, again):
+        assert a["eps_r"] == b["eps_r"] and np.array_equal(a["mesh"].points, b["mesh"].points)
