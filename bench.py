@@ -40,11 +40,13 @@ FREQ = 3.0e8
 def launches_per_apply(max_level: int, tune: dict) -> int:
     """Kernels one operator apply launches: the aggregation (one launch for
     both media with agg variant 1, else one per medium); per medium one
-    interpolation per level pair, the translations (one launch for every
-    level with m2l variants 2-5, else one per level) and one anterpolation per
-    level pair; then the leaf testing + near-field kernel."""
+    interpolation per level pair, the translations (the leaf level and the
+    other levels as two launches with m2l variants 2-5, else one per level)
+    and one anterpolation per level pair; then the leaf testing + near-field
+    kernel."""
     lv = max_level - 2
-    m2l = 1 if tune["m2l.variant"] in (2, 3, 4, 5) else lv + 1
+    # segmented translation variants: the leaf level and the other levels as two launches
+    m2l = 2 if tune["m2l.variant"] in (2, 3, 4, 5) else lv + 1
     agg = 1 if tune.get("agg.variant", 0) == 1 else 2
     return agg + 2 * (lv + m2l + lv) + 1
 
@@ -532,7 +534,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["product", "reference"], default="product")
     ap.add_argument("--size", choices=["full", "mid", "small"], default="full")
-    ap.add_argument("--solve-its", type=int, default=1000, help="outer iteration cap of the solve")
+    ap.add_argument("--solve-its", type=int, default=300, help="outer iteration cap of the solves")
     ap.add_argument("--inner-its", type=int, default=16, help="near-field GMRES steps per preconditioning")
     ap.add_argument("--plain-its", type=int, default=300, help="iteration cap of the plain GMRES comparison")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference matvecs to time")

@@ -1183,14 +1183,14 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
   }
 }
 
-// Translations of every level of medium m (independent of each other).
-void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
-  const int L = P.maxL;
+// Translations of levels lo..hi of medium m (independent of each other).
+void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s, int lo, int hi) {
+  if (lo > hi) return;
   if (P.tuning.m2l_variant == 4 || P.tuning.m2l_variant == 5) {
-    if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+    if (hi - lo + 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
     M2lPairArg<double2> a{};
     int ctas = 0;
-    for (int l = 2; l <= L; ++l) {
+    for (int l = lo; l <= hi; ++l) {
       const MediumLevel& cm = P.ml[m][l];
       M2lPairSeg<double2>& g = a.seg[a.nseg++];
       g = M2lPairSeg<double2>{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, P.lv[l].pair_ptr, P.lv[l].pair_src,
@@ -1205,10 +1205,10 @@ void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
     return;
   }
   if (P.tuning.m2l_variant == 3) {
-    if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+    if (hi - lo + 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
     M2lWarpArg<double2> a{};
     int ctas = 0;
-    for (int l = 2; l <= L; ++l) {
+    for (int l = lo; l <= hi; ++l) {
       const MediumLevel& cm = P.ml[m][l];
       M2lWarpSeg<double2>& g = a.seg[a.nseg++];
       g = M2lWarpSeg<double2>{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, P.lv[l].far_ptr, P.lv[l].far_idx,
@@ -1219,10 +1219,10 @@ void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
     return;
   }
   if (P.tuning.m2l_variant == 2) {
-    if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+    if (hi - lo + 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
     M2lOctArg a{};
     int ctas = 0;
-    for (int l = 2; l <= L; ++l) {
+    for (int l = lo; l <= hi; ++l) {
       const MediumLevel& cm = P.ml[m][l];
       M2lSeg& g = a.seg[a.nseg++];
       g = M2lSeg{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, cm.off2vec, P.lv[l].ufar_ptr, P.lv[l].ufar,
@@ -1233,7 +1233,7 @@ void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s) {
     m2l_oct_kernel<<<ctas, kM2lThreads, 0, s>>>(a);
     return;
   }
-  for (int l = 2; l <= L; ++l) {
+  for (int l = lo; l <= hi; ++l) {
     const MediumLevel& cm = P.ml[m][l];
     if (P.tuning.m2l_variant == 1) {
       M2lTileArg a{level_S(P, m, l, v), level_B(P, m, l, v), P.lv[l - 1].child_begin, P.lv[l].usrc_ptr,
@@ -1325,13 +1325,37 @@ cudaEvent_t* profiler_events(Plan& P, cudaStream_t s) {
 }
 
 // The tree passes of medium m with fixed kernel choices (interpolation 0,
-// translation 3, anterpolation 1) for either storage type; leafS / leafB are
-// the leaf-level arrays (the plan's own or one batch slot).
+// translation 4, anterpolation 1) for either storage type; leafS / leafB are
+// the leaf-level arrays (the plan's own or one batch slot). With a leaf
+// stream sx, the leaf level's translation runs there after the aggregation
+// (ev_agg) while the interpolation climbs the tree on s; s waits for it
+// (ev_leaf) before the anterpolation chain.
 template <class C>
-void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s) {
+void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s, cudaStream_t sx = nullptr,
+                     cudaEvent_t ev_agg = nullptr, cudaEvent_t ev_leaf = nullptr) {
   const int L = P.maxL;
   auto S_at = [&](int l) -> C* { return l == L ? leafS : Store<C>::S(P.ml[m][l]); };
   auto B_at = [&](int l) -> C* { return l == L ? leafB : Store<C>::Bm(P.ml[m][l]); };
+  auto translate = [&](int lo, int hi, cudaStream_t st) {
+    if (lo > hi) return;
+    if (hi - lo + 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+    M2lPairArg<C> t{};
+    int ctas = 0;
+    for (int l = lo; l <= hi; ++l) {
+      const MediumLevel& cm = P.ml[m][l];
+      M2lPairSeg<C>& g = t.seg[t.nseg++];
+      g = M2lPairSeg<C>{S_at(l),          B_at(l),   Store<C>::tfw(cm), P.lv[l].pair_ptr, P.lv[l].pair_src,
+                        P.lv[l].pair_vec, P.lv[l].B, cm.K,              (cm.K + 31) / 32, ctas};
+      ctas += (((P.lv[l].B + 1) / 2 + kPairWarps - 1) / kPairWarps) * g.nchunk;
+    }
+    m2l_pair_kernel<C><<<ctas, 32 * kPairWarps, 0, st>>>(t);
+  };
+  if (sx) {
+    MLFMA_CUDA(cudaEventRecord(ev_agg, s));
+    MLFMA_CUDA(cudaStreamWaitEvent(sx, ev_agg, 0));
+    translate(L, L, sx);
+    MLFMA_CUDA(cudaEventRecord(ev_leaf, sx));
+  }
   for (int l = L - 1; l >= 2; --l) {
     const MediumLevel& pm = P.ml[m][l];
     const MediumLevel& cm = P.ml[m][l + 1];
@@ -1339,17 +1363,12 @@ void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s) {
                Store<C>::ph_up(pm), pm.K, pm.nph, cm.K, cm.nph};
     up_kernel<C><<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6), kThreads, 0, s>>>(a);
   }
-  if (L - 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
-  M2lWarpArg<C> t{};
-  int ctas = 0;
-  for (int l = 2; l <= L; ++l) {
-    const MediumLevel& cm = P.ml[m][l];
-    M2lWarpSeg<C>& g = t.seg[t.nseg++];
-    g = M2lWarpSeg<C>{S_at(l),         B_at(l), Store<C>::tfw(cm), P.lv[l].far_ptr, P.lv[l].far_idx, P.lv[l].far_vec,
-                      P.lv[l].B,       cm.K,    (cm.K + 31) / 32,   ctas};
-    ctas += ((P.lv[l].B + kWarpBoxes - 1) / kWarpBoxes) * g.nchunk;
+  if (sx) {
+    translate(2, L - 1, s);
+    MLFMA_CUDA(cudaStreamWaitEvent(s, ev_leaf, 0));
+  } else {
+    translate(2, L, s);
   }
-  m2l_warp_kernel<C><<<ctas, 32 * kWarpBoxes, 0, s>>>(t);
   for (int l = 3; l <= L; ++l) {
     const MediumLevel& cm = P.ml[m][l];
     const MediumLevel& pm = P.ml[m][l - 1];
@@ -1371,7 +1390,7 @@ void apply_fixed(Plan& P, const double2* x, double2* w, cudaStream_t s) {
     const MediumLevel& leaf = P.ml[m][L];
     agg_kernel<C><<<dim3(P.lv[L].B, (leaf.K + kThreads - 1) / kThreads), kThreads, 0, sm>>>(
         Store<C>::Vs(P, m), P.d_leaf_ptr, P.d_leaf_rwg, x, P.N, leaf.K, Store<C>::S(leaf));
-    tree_pass_fixed<C>(P, m, Store<C>::S(leaf), Store<C>::Bm(leaf), sm);
+    tree_pass_fixed<C>(P, m, Store<C>::S(leaf), Store<C>::Bm(leaf), sm, P.stream_leaf[m], P.ev_agg[m], P.ev_leaf[m]);
     a.Vf[m] = Store<C>::Vf(P, m);
     a.Bm[m] = Store<C>::Bm(leaf);
     a.khat[m] = leaf.khat;
@@ -1460,12 +1479,27 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
     }
     if (ev) MLFMA_CUDA(cudaEventRecord(ev[1 + 4 * m], s));
     const LeafView v{leaf.S, leaf.Bm};
+    if (ev) {  // one stage after the other, for the stage events
+      launch_up(P, m, v, s);
+      MLFMA_CUDA(cudaEventRecord(ev[2 + 4 * m], s));
+      launch_m2l(P, m, v, s, 2, L);
+      MLFMA_CUDA(cudaEventRecord(ev[3 + 4 * m], s));
+      launch_l2l(P, m, v, s);
+      MLFMA_CUDA(cudaEventRecord(ev[4 + 4 * m], s));
+      continue;
+    }
+    // The leaf level's translation needs only the aggregation: it runs on a
+    // stream of its own while the interpolation climbs the tree; the
+    // anterpolation chain starts once both are done.
+    const cudaStream_t sx = P.stream_leaf[m];
+    MLFMA_CUDA(cudaEventRecord(P.ev_agg[m], sm));
+    MLFMA_CUDA(cudaStreamWaitEvent(sx, P.ev_agg[m], 0));
+    launch_m2l(P, m, v, sx, L, L);
+    MLFMA_CUDA(cudaEventRecord(P.ev_leaf[m], sx));
     launch_up(P, m, v, sm);
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[2 + 4 * m], s));
-    launch_m2l(P, m, v, sm);
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[3 + 4 * m], s));
+    launch_m2l(P, m, v, sm, 2, L - 1);
+    MLFMA_CUDA(cudaStreamWaitEvent(sm, P.ev_leaf[m], 0));
     launch_l2l(P, m, v, sm);
-    if (ev) MLFMA_CUDA(cudaEventRecord(ev[4 + 4 * m], s));
   }
   ms.join();
   LeafArg<double2> a{};
@@ -1526,7 +1560,7 @@ void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2
         for (int m = 0; m < 2; ++m) {
           const LeafView v{P.bS[m][j], P.bB[m][j]};
           launch_up(P, m, v, ms.of(m));
-          launch_m2l(P, m, v, ms.of(m));
+          launch_m2l(P, m, v, ms.of(m), 2, P.maxL);
           launch_l2l(P, m, v, ms.of(m));
         }
       ms.join();

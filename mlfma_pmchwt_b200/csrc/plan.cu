@@ -29,6 +29,14 @@ Plan::~Plan() {
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    for (int m = 0; m < 2; ++m) {
+      if (stream_leaf[m]) {
+        cudaStreamSynchronize(stream_leaf[m]);
+        cudaStreamDestroy(stream_leaf[m]);
+      }
+      if (ev_agg[m]) cudaEventDestroy(ev_agg[m]);
+      if (ev_leaf[m]) cudaEventDestroy(ev_leaf[m]);
+    }
   }
 }
 
@@ -141,6 +149,11 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   MLFMA_CUDA(cudaStreamCreateWithFlags(&P->stream2, cudaStreamNonBlocking));
   MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
   MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
+  for (int m = 0; m < 2; ++m) {
+    MLFMA_CUDA(cudaStreamCreateWithFlags(&P->stream_leaf[m], cudaStreamNonBlocking));
+    MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_agg[m], cudaEventDisableTiming));
+    MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_leaf[m], cudaEventDisableTiming));
+  }
   cudaStream_t s = P->stream;
   const Mesh& Me = P->mesh;
   const Rwg& R = P->rwg;

@@ -195,6 +195,10 @@ struct Plan {
   // back into the caller's stream with these events
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // per medium: the leaf level's translation runs on stream_leaf[m] after
+  // ev_agg[m] (aggregation done); ev_leaf[m] marks its end
+  cudaStream_t stream_leaf[2] = {nullptr, nullptr};
+  cudaEvent_t ev_agg[2] = {nullptr, nullptr}, ev_leaf[2] = {nullptr, nullptr};
   StageProfiler prof;
   size_t bytes = 0;
   std::vector<void*> allocations;
@@ -293,7 +297,7 @@ void reserve_batch(Plan& P, int R);  // allocates the leaf-level arrays of min(R
 void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw, cudaStream_t s);
 // The complex64 operator (precision = mixed plans): complex128 x and w, every
 // table and workspace in complex64, FP32 arithmetic. Fixed kernel choices:
-// aggregation 0, interpolation 0, translation 3, anterpolation 1.
+// aggregation 0, interpolation 0, translation 4, anterpolation 1.
 void apply_mixed_device(Plan& P, const double2* x, double2* w, cudaStream_t s);
 void apply_batch_mixed_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw,
                               cudaStream_t s);
