@@ -840,7 +840,7 @@ inline int l2l_grid_y(int boxes, int ntc, int npp) {
 // reference's 9-tap weight of a (parent, child) direction pair is the
 // product of the two 1-D weights used here (Code/AlgoMLFMM.h:347-351).
 template <class C>
-__global__ void __launch_bounds__(256) l2l_sep_kernel(L2lSepArg<C> a) {
+__global__ void __launch_bounds__(256, 4) l2l_sep_kernel(L2lSepArg<C> a) {
   using R = typename Cx<C>::real;
   __shared__ C band[kL2lBand];
   const int b = blockIdx.x;

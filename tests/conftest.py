@@ -51,6 +51,10 @@ CASES = {
     # deep trees (maxLevel 5) at small cost: small leaf boxes
     "sphere_s4_deep": (lambda: M.icosphere(4, 1.5), 2.5 - 0.1j, 0.12),
     "ellipsoid_s4_deep": (lambda: M.ellipsoid(4, 2.0, 1.4, 1.0), 4.0, 0.15),
+    # the smallest trees (maxLevel 2): no interpolation levels; and one whose
+    # boxes are all near each other (no interaction pairs: near field only)
+    "sphere_s2_flat": (lambda: M.icosphere(2, 0.3), 4.0, 0.25),
+    "sphere_s1_allnear": (lambda: M.icosphere(1, 0.2), complex(2.5, -0.1), 0.3),
 }
 
 

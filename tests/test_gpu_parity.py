@@ -28,7 +28,8 @@ def gpu_op(case_files, name):
     return _ops[name]
 
 
-CASES = ["sphere_s2", "sphere_s3", "sphere_s3_lossy", "ellipsoid_s3", "sphere_s4_deep", "ellipsoid_s4_deep"]
+CASES = ["sphere_s2", "sphere_s3", "sphere_s3_lossy", "ellipsoid_s3", "sphere_s4_deep", "ellipsoid_s4_deep",
+         "sphere_s2_flat", "sphere_s1_allnear"]
 
 
 @pytest.mark.parametrize("name", CASES)

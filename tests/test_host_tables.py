@@ -8,7 +8,8 @@ import pytest
 
 from conftest import FREQ, needs_lib, needs_oracle
 
-HOST_CASES = ["sphere_s2", "sphere_s3", "sphere_s3_lossy", "ellipsoid_s3", "sphere_s4_deep", "ellipsoid_s4_deep"]
+HOST_CASES = ["sphere_s2", "sphere_s3", "sphere_s3_lossy", "ellipsoid_s3", "sphere_s4_deep", "ellipsoid_s4_deep",
+              "sphere_s2_flat", "sphere_s1_allnear"]
 
 
 def host_plan(case_files, name):
