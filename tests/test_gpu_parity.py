@@ -50,8 +50,10 @@ def test_transfer_factors(case_files, ref_ops, name):
             box = ref.level(lvl)["length"][0]
             roffs = np.rint(rvec / box).astype(int)
             assert {tuple(o) for o in offs} == {tuple(o) for o in roffs}
+            if len(roffs) == 0:  # no interaction pairs on this level
+                continue
             where = {tuple(o): i for i, o in enumerate(offs)}
-            sel = np.array([where[tuple(o)] for o in roffs])
+            sel = np.array([where[tuple(o)] for o in roffs], dtype=int)
             assert rel(tf[sel], rtf) < TABLE_TOL, (med, lvl)
 
 
