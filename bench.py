@@ -41,14 +41,15 @@ def launches_per_apply(max_level: int, tune: dict) -> int:
     """Kernels one operator apply launches: the aggregation (one launch for
     both media with agg variant 1, else one per medium); per medium one
     interpolation per level pair, the translations (the leaf level and the
-    other levels as two launches with m2l variants 2-5, else one per level)
+    other levels as two launches with m2l variants 2-7, else one per level)
     and one anterpolation per level pair; then the leaf testing + near-field
-    kernel."""
+    kernel (two kernels with leaf variant 1)."""
     lv = max_level - 2
     # segmented translation variants: the leaf level and the other levels as two launches
-    m2l = 2 if tune["m2l.variant"] in (2, 3, 4, 5) else lv + 1
+    m2l = 2 if tune["m2l.variant"] in (2, 3, 4, 5, 6, 7, 8) else lv + 1
     agg = 1 if tune.get("agg.variant", 0) == 1 else 2
-    return agg + 2 * (lv + m2l + lv) + 1
+    leaf = 2 if tune.get("leaf.variant", 0) == 1 else 1
+    return agg + 2 * (lv + m2l + lv) + leaf
 
 
 def workload(args):

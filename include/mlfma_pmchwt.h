@@ -129,6 +129,12 @@ MLFMA_API int mlfma_apply(mlfma_plan* plan, int n, const double* x, double* w);
  * (cudaStream_t passed as void*; NULL = the plan's stream). Asynchronous. */
 MLFMA_API int mlfma_apply_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream);
 
+/* Device status bits of a plan after the device-pointer calls: synchronizes
+ * the device and writes 0, or 1 when a bounded wait of the staged
+ * translation (m2l.variant 6, 7) ran out and its output is not valid. The
+ * host-pointer calls check the same bits and fail with MLFMA_ERR_CUDA. */
+MLFMA_API int mlfma_device_status(mlfma_plan* plan, int* status);
+
 /* Batched apply: w[j] = A x[j] for R right-hand sides stored one after the
  * other (x[j] at x + 2 n j doubles, complex128 interleaved, n = 2N each).
  * The reference applies its AxFunc (Code/GMRES.h:53-66, the ax closure of
@@ -150,34 +156,45 @@ MLFMA_API int mlfma_apply_batch_device(mlfma_plan* plan, int n, int R, const voi
 MLFMA_API int mlfma_profile(mlfma_plan* plan, int on);
 MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applies);
 
-/* Kernel variants of a plan (no counterpart in the reference). Keys and values:
- *   "m2l.variant"  0 = one thread per (box, direction) over the interaction
- *                  list; 1 = sibling-group tiles staging the shared sources in
- *                  shared memory; 2 = octant registers: one thread per
- *                  (parent, direction, J|M) holds all 8 children and applies
- *                  each source of the siblings' union once, every level of a
- *                  medium in one launch; 3 = warp per box, 8 Morton-consecutive
- *                  boxes per CTA sharing their source patterns through L1, every
- *                  level of a medium in one launch; 4 = warp per pair of
- *                  Morton-consecutive boxes over their merged lists (each source
- *                  pattern loaded once for both), every level in one launch;
- *                  5 = the same with J and M halves on separate warps.
- *   "up.variant"   0 = 9-tap gather per parent direction; 1 = separable
- *                  phi-then-theta interpolation in bands of theta rows (default);
- *                  2 = one thread per (parent, direction) for all 6 components;
- *                  3 = separable in registers: a thread takes a phi column of a
- *                  band of 4 parent theta rows.
- *   "l2l.variant"  0 = transposed 9-tap gather per child direction;
- *                  1 = separable transposed theta-then-phi (default).
- *   "agg.variant"  0 = one thread per (leaf box, direction), one launch per
- *                  medium; 1 = one CTA per (leaf box, medium) streaming the
- *                  box's contiguous pattern block, both media in one launch
- *                  (default).
+/* Kernel variants of a plan (no counterpart in the reference). Keys, values
+ * and defaults (the fastest measured at 245,760 unknowns):
+ *   "m2l.variant"  translation: 0 = one thread per (box, direction) over the
+ *                  interaction list; 1 = sibling-group tiles staging the shared
+ *                  sources in shared memory; 2 = octant registers over the
+ *                  siblings' union; 3 = warp per box, 8 Morton-consecutive
+ *                  boxes per CTA; 4 = warp per pair of Morton-consecutive boxes
+ *                  over their merged lists, each source pattern loaded once for
+ *                  both (default); 5 = as 4 with the J and M halves on separate
+ *                  warps; 6 = groups of 8 Morton-consecutive boxes over the
+ *                  union of their lists, each union source's patterns staged
+ *                  in shared memory by bulk asynchronous copies ahead of the
+ *                  arithmetic, 2 boxes per warp; 7 = as 6 with 4 boxes per
+ *                  warp. 2-7 launch the leaf level and the other levels of a
+ *                  medium as two launches.
+ *   "up.variant"   interpolation: 0 = 9-tap gather per parent direction and
+ *                  component (default); 1 = separable phi-then-theta in bands of
+ *                  theta rows through shared memory; 2 = one thread per
+ *                  (parent, direction) for all 6 components; 3 = separable in
+ *                  registers, a phi column of 4 parent theta rows per thread.
+ *   "l2l.variant"  anterpolation: 0 = transposed 9-tap gather per child
+ *                  direction; 1 = separable transposed theta-then-phi (default).
+ *   "agg.variant"  aggregation: 0 = one thread per (leaf box, direction), one
+ *                  launch per medium (default); 1 = one CTA per (leaf box,
+ *                  medium) streaming the box's contiguous pattern block.
+ *   "leaf.variant" 0 = the near-field rows inside the leaf testing kernel (default);
+ *                  1 = the near-field product on its own stream from the start
+ *                  of the apply (it needs only x), overlapping the tree
+ *                  passes; the leaf kernel then adds the far field.
+ *   "apply.graph"  1 = each apply (per x, w, stream and precision) is captured
+ *                  as a CUDA graph on first use and replayed afterwards
+ *                  (default); 0 = direct launches. Setting any key drops the
+ *                  captured graphs. The first apply with given pointers should
+ *                  come before the caller captures its own graph.
  * mlfma_autotune times the values of each key in that order (the others held
  * at their current values) over `applies` applies of the plan's own operator
  * (device vectors owned by the plan) and keeps the fastest; variant_ms (may be
  * NULL) receives the per-apply ms of every value, keys in that order
- * (14 entries: m2l 0-5, up 0-3, l2l 0-1, agg 0-1). */
+ * (21 entries: m2l 0-8, up 0-3, l2l 0-1, agg 0-1, leaf 0-1, graph 0-1). */
 MLFMA_API int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value);
 MLFMA_API int mlfma_get_tuning(const mlfma_plan* plan, const char* key);
 MLFMA_API int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms);

@@ -78,6 +78,7 @@ SIGNATURES = {
     "mlfma_plan_info": (C.c_int, [_P, C.POINTER(Info)]),
     "mlfma_apply": (C.c_int, [_P, C.c_int, _DP, _DP]),
     "mlfma_apply_device": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "mlfma_device_status": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "mlfma_apply_batch": (C.c_int, [_P, C.c_int, C.c_int, _DP, _DP]),
     "mlfma_apply_batch_device": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P]),
     "mlfma_profile": (C.c_int, [_P, C.c_int]),
@@ -278,6 +279,13 @@ class MLFMM:
         self._check(self._lib.mlfma_apply_device(self._h, self.n, C.c_void_p(x_ptr), C.c_void_p(w_ptr),
                                                  C.c_void_p(stream or 0)))
 
+    def device_status(self) -> int:
+        """Synchronizes the device; 0, or the status bits a kernel recorded
+        (1: a bounded wait of the staged translation ran out)."""
+        st = C.c_int(0)
+        self._check(self._lib.mlfma_device_status(self._h, C.byref(st)))
+        return st.value
+
     def apply_batch(self, X) -> np.ndarray:
         """W[j] = A X[j] for the rows of X (host, complex128 [R, 2N]); patterns
         and near-field entries are read once per group of 16 right-hand sides."""
@@ -300,7 +308,7 @@ class MLFMM:
     def get_tuning(self, key: str) -> int:
         return self._check(self._lib.mlfma_get_tuning(self._h, key.encode()))
 
-    TUNING_KEYS = (("m2l.variant", 6), ("up.variant", 4), ("l2l.variant", 2), ("agg.variant", 2))
+    TUNING_KEYS = (("m2l.variant", 9), ("up.variant", 4), ("l2l.variant", 2), ("agg.variant", 2), ("leaf.variant", 2), ("apply.graph", 2))
 
     def autotune(self, applies: int = 3) -> dict:
         """Times the values of each tuning key on this plan (one key at a

@@ -61,6 +61,16 @@ mlfma::PlanParams to_params(const mlfma_params* p) {
 
 bool device_plan(const mlfma_plan* plan) { return plan && plan->p && plan->p->device >= 0; }
 
+// Waits for the plan's stream and raises if a kernel recorded a device
+// status bit (a bounded wait of the staged translation that ran out).
+void sync_and_check(mlfma::Plan& P) {
+  MLFMA_CUDA(cudaMemcpyAsync(P.h_status, P.d_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+  MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+  if (*P.h_status != 0)
+    throw mlfma::CudaError("device status " + std::to_string(*P.h_status) +
+                           ": a bounded wait in the staged translation ran out");
+}
+
 }  // namespace
 
 extern "C" {
@@ -161,7 +171,19 @@ int mlfma_apply(mlfma_plan* plan, int n, const double* x, double* w) {
     MLFMA_CUDA(cudaMemcpyAsync(P.d_x, x, bytes, cudaMemcpyHostToDevice, P.stream));
     mlfma::apply_device(P, P.d_x, P.d_w, P.stream);
     MLFMA_CUDA(cudaMemcpyAsync(w, P.d_w, bytes, cudaMemcpyDeviceToHost, P.stream));
-    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    sync_and_check(P);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_device_status(mlfma_plan* plan, int* status) {
+  if (!plan || !plan->p || !status) return fail(MLFMA_ERR_ARG, "null argument");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    MLFMA_CUDA(cudaDeviceSynchronize());
+    MLFMA_CUDA(cudaMemcpy(status, P.d_status, sizeof(int), cudaMemcpyDeviceToHost));
     return MLFMA_OK;
   });
 }
@@ -203,7 +225,7 @@ int mlfma_apply_batch(mlfma_plan* plan, int n, int R, const double* x, double* w
       MLFMA_CUDA(cudaMemcpyAsync(w + 2 * static_cast<size_t>(g0) * n, P.d_wb, bytes, cudaMemcpyDeviceToHost,
                                  P.stream));
     }
-    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    sync_and_check(P);
     return MLFMA_OK;
   });
 }
@@ -250,10 +272,12 @@ struct TuningKey {
   int count;  // values 0 .. count-1
 };
 constexpr TuningKey kTuningKeys[] = {
-    {"m2l.variant", &mlfma::Tuning::m2l_variant, 6},
+    {"m2l.variant", &mlfma::Tuning::m2l_variant, 9},
     {"up.variant", &mlfma::Tuning::up_variant, 4},
     {"l2l.variant", &mlfma::Tuning::l2l_variant, 2},
     {"agg.variant", &mlfma::Tuning::agg_variant, 2},
+    {"leaf.variant", &mlfma::Tuning::leaf_variant, 2},
+    {"apply.graph", &mlfma::Tuning::graph, 2},
 };
 const TuningKey* find_key(const char* key) {
   for (const TuningKey& k : kTuningKeys)
@@ -269,6 +293,7 @@ int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value) {
   if (value < 0 || value >= k->count)
     return fail(MLFMA_ERR_ARG, std::string(key) + " must be in [0, " + std::to_string(k->count - 1) + "]");
   plan->p->tuning.*(k->field) = value;
+  if (device_plan(plan)) mlfma::clear_graphs(*plan->p);
   return MLFMA_OK;
 }
 
@@ -297,6 +322,7 @@ int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
       for (int i = 0; i < applies; ++i) mlfma::apply_device(P, P.d_x, P.d_w, P.stream);
       MLFMA_CUDA(cudaEventRecord(e1, P.stream));
       MLFMA_CUDA(cudaEventSynchronize(e1));
+      sync_and_check(P);
       float ms = 0.f;
       MLFMA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       return static_cast<double>(ms) / applies;
@@ -308,6 +334,7 @@ int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
       int best_v = P.tuning.*(k.field);
       for (int v = 0; v < k.count; ++v) {
         P.tuning.*(k.field) = v;
+        mlfma::clear_graphs(P);
         const double per = time_apply();
         if (variant_ms) variant_ms[slot + v] = per;
         if (per < best) {
@@ -316,6 +343,7 @@ int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
         }
       }
       P.tuning.*(k.field) = best_v;
+      mlfma::clear_graphs(P);
       slot += k.count;
     }
     P.prof.on = prof;

@@ -13,11 +13,20 @@
 // Every stage writes its output before anything accumulates into it (l2l adds
 // onto the Bm that m2l of the same level has just written), so no clearing
 // pass (Code/ProcessMLFMM.h:14-28) is needed.
-#include <algorithm>
-#include <type_traits>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <utility>
+
+#include "bulk.cuh"
 #include "cplx.cuh"
 #include "plan.hpp"
+#include "solver.hpp"
 
 namespace mlfma {
 
@@ -801,6 +810,255 @@ __global__ void __launch_bounds__(64 * kPairWarps) m2l_pairh_kernel(const __grid
   }
 }
 
+// Translation with staged sources: a CTA takes a group of 8 Morton-
+// consecutive boxes and 32 directions. The group's interaction lists are
+// merged into one source-ordered union whose entries carry the transfer-
+// factor row of each member that lists the source. A producer warp stages,
+// per union entry, the source's 6 pattern rows (one tiled TMA copy of a
+// 6-row box) and the listed members' transfer-factor rows (two tile::gather4
+// copies of 4 rows each) for 32 directions into a ring of shared-memory
+// stages, completing on the stage's mbarrier, kGrpStages entries ahead of the
+// arithmetic. kGrpBoxes / kBW compute warps, one direction per lane, apply
+// every staged entry to their kBW boxes from shared memory only: no compute
+// warp waits on a global load. A source pattern crosses L2 once per group
+// instead of once per box pair. Each box still sums its sources in ascending
+// order.
+constexpr int kGrpBoxes = 8;
+constexpr int kGrpDirs = 32;
+constexpr int kGrpStages = 6;
+constexpr int kGrpRows = 6 + kGrpBoxes;  // staged rows per entry: 6 pattern components, 8 transfer factors
+constexpr int kGrpMaxSeg = 8;            // levels per launch
+
+template <class C>
+struct M2lGrpSeg {
+  CUtensorMap smap;  // the level's patterns as rows [B * 6][2K] of scalars, box 2 * kGrpDirs x 6
+  const C* S;
+  const C* tfw;
+  C* Bm;
+  const int* grp_ptr;
+  const int* grp_src;
+  const int4* grp_code;
+  int B, K, G, nchunk, cta_begin;
+};
+template <class C>
+struct M2lGrpArg {
+  M2lGrpSeg<C> seg[kGrpMaxSeg];
+  int nseg;
+  int* status;
+};
+
+template <class C>
+constexpr size_t grp_smem_bytes() {
+  return static_cast<size_t>(kGrpStages) * kGrpRows * kGrpDirs * sizeof(C) + kGrpStages * sizeof(int4) +
+         2 * kGrpStages * sizeof(uint64_t);
+}
+
+__device__ __forceinline__ int grp_field(const int4& w, int j) {
+  const int v = (j >> 1) == 0 ? w.x : (j >> 1) == 1 ? w.y : (j >> 1) == 2 ? w.z : w.w;
+  return (j & 1) ? (v >> 16) : static_cast<int>(static_cast<short>(v & 0xffff));
+}
+
+template <class C, int kBW, bool kTmaS>
+__global__ void __launch_bounds__(32 * (kGrpBoxes / kBW + 1)) m2l_grp_kernel(const __grid_constant__ M2lGrpArg<C> a) {
+  constexpr int kCW = kGrpBoxes / kBW;  // compute warps; warp kCW is the producer
+  constexpr uint32_t kRowBytes = kGrpDirs * sizeof(C);
+  extern __shared__ __align__(128) unsigned char smem[];
+  C* stage = reinterpret_cast<C*>(smem);  // [kGrpStages][kGrpRows][kGrpDirs]
+  int4* codes = reinterpret_cast<int4*>(smem + static_cast<size_t>(kGrpStages) * kGrpRows * kRowBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(codes + kGrpStages);
+  uint64_t* empty = full + kGrpStages;
+
+  int si = 0;
+  while (si + 1 < a.nseg && static_cast<int>(blockIdx.x) >= a.seg[si + 1].cta_begin) ++si;
+  const M2lGrpSeg<C>& g = a.seg[si];
+  const int local = blockIdx.x - g.cta_begin;
+  const int chunk = local / g.G, grp = local - chunk * g.G;
+  const int k0 = chunk * kGrpDirs;
+  const int nk = min(kGrpDirs, g.K - k0);
+  const int e0 = g.grp_ptr[grp], n = g.grp_ptr[grp + 1] - e0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (status_now(a.status) != 0) return;  // an earlier wait ran out: the output is void anyway
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kGrpStages; ++i) {
+      mbar_init(full + i, 33);  // the producer's 32 lanes after their copies, and lane 0 with the codes
+      mbar_init(empty + i, kCW);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+
+  if (warp == kCW) {  // producer
+    if (kTmaS && lane == 0) tma_prefetch_map(&g.smap);
+    bool ok = true;
+    int i = 0;
+    for (int base = 0; base < n && ok; base += 32) {
+      int src = 0;
+      int4 cd = make_int4(-1, -1, -1, -1);
+      if (base + lane < n) {
+        src = __ldg(g.grp_src + e0 + base + lane);
+        cd = __ldg(g.grp_code + e0 + base + lane);
+      }
+      const int cnt = min(32, n - base);
+      for (int j = 0; j < cnt; ++j, ++i) {
+        const int sj = __shfl_sync(0xffffffffu, src, j);
+        const int4 cj = make_int4(__shfl_sync(0xffffffffu, cd.x, j), __shfl_sync(0xffffffffu, cd.y, j),
+                                  __shfl_sync(0xffffffffu, cd.z, j), __shfl_sync(0xffffffffu, cd.w, j));
+        const int st = i % kGrpStages;
+        const bool waited = i < kGrpStages || mbar_wait(empty + st, ((i / kGrpStages) - 1) & 1, a.status);
+        if (!__all_sync(0xffffffffu, waited)) {
+          ok = false;
+          break;
+        }
+        C* dst = stage + st * kGrpRows * kGrpDirs;
+        if (lane == 0) {  // the codes, released to the compute warps by this arrival
+          codes[st] = cj;
+          if (kTmaS) {
+            mbar_arrive_expect_tx(full + st, 6 * kRowBytes);
+            tma_load_2d(dst, &g.smap, 2 * k0, 6 * sj, full + st);
+          } else {
+            mbar_arrive(full + st);
+          }
+        }
+        if (lane < nk) {
+          if (!kTmaS) {
+            const C* p = g.S + static_cast<size_t>(sj) * 6 * g.K + k0 + lane;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) cp_async_ca<sizeof(C)>(dst + c * kGrpDirs + lane, p + static_cast<size_t>(c) * g.K);
+          }
+#pragma unroll
+          for (int b = 0; b < kGrpBoxes; ++b) {
+            const int code = grp_field(cj, b);
+            if (code >= 0)
+              cp_async_ca<sizeof(C)>(dst + (6 + b) * kGrpDirs + lane, g.tfw + static_cast<size_t>(code) * g.K + k0 + lane);
+          }
+        }
+        cp_async_arrive(full + st);
+      }
+    }
+    // the copies still in flight land before the producer leaves, so that the
+    // CTA never ends (a compute warp may give up after a failed wait) with a
+    // copy into its shared memory outstanding
+    if (lane == 0)
+      for (int q = max(0, i - kGrpStages); q < i; ++q)
+        mbar_wait(full + q % kGrpStages, (q / kGrpStages) & 1, a.status, false);
+    return;
+  }
+
+  const int k = k0 + lane;
+  C acc[kBW][6];
+#pragma unroll
+  for (int j = 0; j < kBW; ++j)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[j][c] = Cx<C>::zero();
+  bool ok = true;
+  for (int i = 0; i < n; ++i) {
+    const int st = i % kGrpStages;
+    if (!mbar_wait(full + st, (i / kGrpStages) & 1, a.status)) {
+      ok = false;
+      break;
+    }
+    const int4 cw = codes[st];
+    const C* sp = stage + st * kGrpRows * kGrpDirs + lane;
+    int cc[kBW];
+    C t[kBW];
+#pragma unroll
+    for (int j = 0; j < kBW; ++j) {
+      cc[j] = grp_field(cw, warp * kBW + j);
+      t[j] = sp[(6 + warp * kBW + j) * kGrpDirs];  // not used when cc[j] < 0
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      const C sv = sp[c * kGrpDirs];
+#pragma unroll
+      for (int j = 0; j < kBW; ++j)
+        if (cc[j] >= 0) acc[j][c] = cfma(t[j], sv, acc[j][c]);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty + st);
+  }
+  if (!ok || lane >= nk) return;
+#pragma unroll
+  for (int j = 0; j < kBW; ++j) {
+    const int b = grp * kGrpBoxes + warp * kBW + j;
+    if (b < g.B) {
+      C* out = g.Bm + static_cast<size_t>(b) * 6 * g.K + k;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) out[static_cast<size_t>(c) * g.K] = acc[j][c];
+    }
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    MLFMA_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || p == nullptr)
+      throw std::runtime_error("cuTensorMapEncodeTiled is not available from the driver");
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// A 2-D tensor map over rows of K complex values (2K scalars each) with a
+// box of 2 * kGrpDirs scalars by box_rows rows.
+template <class C>
+CUtensorMap rows_tensor_map(const C* base, int K, long long rows, int box_rows) {
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (static_cast<size_t>(K) * sizeof(C)) % 16 != 0)
+    throw std::runtime_error("tensor map: rows not 16-byte aligned");
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {2ull * static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(K) * sizeof(C)};
+  const cuuint32_t box[2] = {2 * kGrpDirs, static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t elem[2] = {1, 1};
+  const CUresult r = tensor_map_encoder()(
+      &m, sizeof(C) == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+      const_cast<C*>(base), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string(r));
+  return m;
+}
+
+// Segments (levels lo..hi) of staged-group translation launches, at most
+// kGrpMaxSeg levels per launch. tf_at(l) gives the level's transfer-factor
+// table and row count.
+template <class C, class SAt, class BAt, class TfAt>
+void launch_m2l_grp(Plan& P, int lo, int hi, int bw, bool tma_s, SAt S_at, BAt B_at, TfAt tf_at, cudaStream_t s) {
+  static_assert(grp_smem_bytes<double2>() <= 48 * 1024, "staged translation needs the opt-in shared memory size");
+  constexpr size_t smem = grp_smem_bytes<C>();
+  for (int l0 = lo; l0 <= hi; l0 += kGrpMaxSeg) {
+    M2lGrpArg<C> a{};
+    a.status = P.d_status;
+    int ctas = 0;
+    for (int l = l0; l <= std::min(hi, l0 + kGrpMaxSeg - 1); ++l) {
+      const auto tf = tf_at(l);  // (table, rows, K)
+      M2lGrpSeg<C>& g = a.seg[a.nseg++];
+      if (tma_s) g.smap = rows_tensor_map<C>(S_at(l), std::get<2>(tf), 6LL * P.lv[l].B, 6);
+      g.S = S_at(l);
+      g.tfw = std::get<0>(tf);
+      g.Bm = B_at(l);
+      g.grp_ptr = P.lv[l].grp_ptr;
+      g.grp_src = P.lv[l].grp_src;
+      g.grp_code = P.lv[l].grp_code;
+      g.B = P.lv[l].B;
+      g.K = std::get<2>(tf);
+      g.G = (P.lv[l].B + kGrpBoxes - 1) / kGrpBoxes;
+      g.nchunk = (g.K + kGrpDirs - 1) / kGrpDirs;
+      g.cta_begin = ctas;
+      ctas += g.G * g.nchunk;
+    }
+    if (tma_s)
+      m2l_grp_kernel<C, 4, true><<<ctas, 32 * (kGrpBoxes / 4 + 1), smem, s>>>(a);
+    else if (bw == 4)
+      m2l_grp_kernel<C, 4, false><<<ctas, 32 * (kGrpBoxes / 4 + 1), smem, s>>>(a);
+    else
+      m2l_grp_kernel<C, 2, false><<<ctas, 32 * (kGrpBoxes / 2 + 1), smem, s>>>(a);
+    MLFMA_CUDA(cudaGetLastError());
+  }
+}
+
 template <class C>
 struct L2lSepArg {
   C* Bm;                 // child level (accumulated into)
@@ -839,6 +1097,7 @@ inline int l2l_grid_y(int boxes, int ntc, int npp) {
 // then by the transposed phi interpolation, and added to the child's Bm. The
 // reference's 9-tap weight of a (parent, child) direction pair is the
 // product of the two 1-D weights used here (Code/AlgoMLFMM.h:347-351).
+// (4 CTAs per SM: 64 registers, up from 3 CTAs at 80.)
 template <class C>
 __global__ void __launch_bounds__(256, 4) l2l_sep_kernel(L2lSepArg<C> a) {
   using R = typename Cx<C>::real;
@@ -919,7 +1178,9 @@ __device__ __forceinline__ C warp_sum(C v) {
 }
 
 // One warp per RWG (leaf order).
-template <class C>
+// kNear = false: the far-field testing only, added to the near-field product
+// already in w (computed concurrently by near_apply).
+template <class C, bool kNear = true>
 __global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg<C> a) {
   using R = typename Cx<C>::real;
   const int lane = threadIdx.x & 31;
@@ -956,20 +1217,22 @@ __global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg<C> a) {
     res[4 * m + 3] = warp_sum(KM);
   }
   // near-field rows t and N + t
-  const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
-  const int tl = r - a.leaf_ptr[b];
-  const C* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
   C nJ = Cx<C>::zero(), nM = Cx<C>::zero();
+  if constexpr (kNear) {
+    const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
+    const int tl = r - a.leaf_ptr[b];
+    const C* Z = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
 #pragma unroll 2
-  for (int j = lane; j < ns; j += 32) {
-    const int s = a.near_src[s0 + j];
-    const C xJ = Cx<C>::from(a.x[s]), xM = Cx<C>::from(a.x[a.N + s]);
-    const C z11 = Z[3 * j], z12 = Z[3 * j + 1], z22 = Z[3 * j + 2];
-    nJ = cfma(z11, xJ, cfma(z12, xM, nJ));
-    nM = cfma(z22, xM, csub(nM, cmul(z12, xJ)));
+    for (int j = lane; j < ns; j += 32) {
+      const int s = a.near_src[s0 + j];
+      const C xJ = Cx<C>::from(a.x[s]), xM = Cx<C>::from(a.x[a.N + s]);
+      const C z11 = Z[3 * j], z12 = Z[3 * j + 1], z22 = Z[3 * j + 2];
+      nJ = cfma(z11, xJ, cfma(z12, xM, nJ));
+      nM = cfma(z22, xM, csub(nM, cmul(z12, xJ)));
+    }
+    nJ = warp_sum(nJ);
+    nM = warp_sum(nM);
   }
-  nJ = warp_sum(nJ);
-  nM = warp_sum(nM);
   if (lane == 0) {
     // w[t]   = c1 (L1J - K1M) + c2 (etai L2J - K2M) + near
     // w[N+t] = c1 (K1J + L1M) + c2 (K2J + L2M / etai) + near
@@ -978,8 +1241,13 @@ __global__ void __launch_bounds__(kThreads) leaf_out_kernel(LeafArg<C> a) {
     wj = cadd(wj, cmul(a.c2, csub(cmul(a.etai, res[4]), res[7])));
     C wm = cmul(a.c1, cadd(res[1], res[2]));
     wm = cadd(wm, cmul(a.c2, cadd(res[5], L2M_eta)));
-    a.w[id] = Cx<C>::to64(cadd(wj, nJ));
-    a.w[a.N + id] = Cx<C>::to64(cadd(wm, nM));
+    if constexpr (kNear) {
+      a.w[id] = Cx<C>::to64(cadd(wj, nJ));
+      a.w[a.N + id] = Cx<C>::to64(cadd(wm, nM));
+    } else {
+      a.w[id] = cadd(a.w[id], Cx<C>::to64(wj));
+      a.w[a.N + id] = cadd(a.w[a.N + id], Cx<C>::to64(wm));
+    }
   }
 }
 
@@ -1186,6 +1454,17 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
 // Translations of levels lo..hi of medium m (independent of each other).
 void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s, int lo, int hi) {
   if (lo > hi) return;
+  if (P.tuning.m2l_variant >= 6) {
+    launch_m2l_grp<double2>(
+        P, lo, hi, P.tuning.m2l_variant == 6 ? 2 : 4, P.tuning.m2l_variant == 8,
+        [&](int l) { return level_S(P, m, l, v); },
+        [&](int l) { return level_B(P, m, l, v); },
+        [&](int l) {
+          return std::make_tuple(static_cast<const double2*>(P.ml[m][l].tfw), P.ml[m][l].nvec, P.ml[m][l].K);
+        },
+        s);
+    return;
+  }
   if (P.tuning.m2l_variant == 4 || P.tuning.m2l_variant == 5) {
     if (hi - lo + 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
     M2lPairArg<double2> a{};
@@ -1311,6 +1590,25 @@ struct MediumStreams {
   }
 };
 
+// The near-field rows need only x: with leaf variant 1 they start at the
+// beginning of the apply on their own stream (writing w), and the leaf
+// kernel adds the far-field testing once they are done.
+struct NearAhead {
+  Plan& P;
+  cudaStream_t s;
+  bool on;
+  NearAhead(Plan& P_, cudaStream_t s_, bool on_, const double2* x, double2* w, int prec) : P(P_), s(s_), on(on_) {
+    if (!on) return;
+    MLFMA_CUDA(cudaEventRecord(P.ev_start, s));
+    MLFMA_CUDA(cudaStreamWaitEvent(P.stream_near, P.ev_start, 0));
+    near_apply(P, x, w, P.stream_near, prec);
+    MLFMA_CUDA(cudaEventRecord(P.ev_near, P.stream_near));
+  }
+  void join() {
+    if (on) MLFMA_CUDA(cudaStreamWaitEvent(s, P.ev_near, 0));
+  }
+};
+
 cudaEvent_t* profiler_events(Plan& P, cudaStream_t s) {
   if (!P.prof.on) return nullptr;
   if (P.prof.used == P.prof.sets.size()) {
@@ -1338,6 +1636,15 @@ void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s, cudaStr
   auto B_at = [&](int l) -> C* { return l == L ? leafB : Store<C>::Bm(P.ml[m][l]); };
   auto translate = [&](int lo, int hi, cudaStream_t st) {
     if (lo > hi) return;
+    if (P.tuning.m2l_variant >= 6) {
+      launch_m2l_grp<C>(
+          P, lo, hi, P.tuning.m2l_variant == 6 ? 2 : 4, P.tuning.m2l_variant == 8, S_at, B_at,
+          [&](int l) {
+            return std::make_tuple(static_cast<const C*>(Store<C>::tfw(P.ml[m][l])), P.ml[m][l].nvec, P.ml[m][l].K);
+          },
+          st);
+      return;
+    }
     if (hi - lo + 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
     M2lPairArg<C> t{};
     int ctas = 0;
@@ -1384,6 +1691,8 @@ template <class C>
 void apply_fixed(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   const int L = P.maxL;
   LeafArg<C> a{};
+  const bool split_near = P.tuning.leaf_variant == 1;
+  NearAhead near(P, s, split_near, x, w, std::is_same<C, float2>::value ? 1 : 0);
   MediumStreams ms(P, s, true);
   for (int m = 0; m < 2; ++m) {
     const cudaStream_t sm = ms.of(m);
@@ -1401,7 +1710,12 @@ void apply_fixed(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   a.x = x;
   a.w = w;
   const int warps = kThreads / 32;
-  leaf_out_kernel<C><<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
+  if (split_near) {
+    near.join();
+    leaf_out_kernel<C, false><<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
+  } else {
+    leaf_out_kernel<C><<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
+  }
   MLFMA_CUDA(cudaGetLastError());
 }
 
@@ -1453,9 +1767,11 @@ void apply_batch_fixed(Plan& P, int R, const double2* X, long long ldx, double2*
 
 }  // namespace
 
-void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
+void apply_direct(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   const int L = P.maxL;
   cudaEvent_t* ev = profiler_events(P, s);
+  const bool split_near = P.tuning.leaf_variant == 1;
+  NearAhead near(P, s, split_near && ev == nullptr, x, w, 0);
   if (P.tuning.agg_variant == 1) {  // both media in one launch, timed as medium 1's aggregation
     AggBoxArg a{};
     for (int m = 0; m < 2; ++m) {
@@ -1513,7 +1829,13 @@ void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   a.x = x;
   a.w = w;
   const int warps = kThreads / 32;
-  leaf_out_kernel<double2><<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
+  if (split_near) {
+    if (ev) near_apply(P, x, w, s, 0);  // profiled: in sequence, inside the leaf stage
+    near.join();
+    leaf_out_kernel<double2, false><<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
+  } else {
+    leaf_out_kernel<double2><<<(P.N + warps - 1) / warps, kThreads, 0, s>>>(a);
+  }
   MLFMA_CUDA(cudaGetLastError());
   if (ev) MLFMA_CUDA(cudaEventRecord(ev[9], s));
 }
@@ -1584,9 +1906,51 @@ void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2
   }
 }
 
+// Replays the captured apply for (x, w, s, precision), capturing it on first
+// use; launches directly while stage profiling, inside another capture, or
+// when the cache is full. Returns false when the caller should launch directly.
+template <class F>
+void apply_graphed(Plan& P, const double2* x, double2* w, cudaStream_t s, int precision, F&& launch) {
+  if (!P.tuning.graph || P.prof.on) return launch();
+  for (const ApplyGraph& g : P.graphs)
+    if (g.x == x && g.w == w && g.s == s && g.precision == precision) {
+      MLFMA_CUDA(cudaGraphLaunch(g.exec, s));
+      return;
+    }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  MLFMA_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone || P.graphs.size() >= kMaxApplyGraphs || s == nullptr) return launch();
+  MLFMA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    launch();
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(s, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  cudaGraph_t graph = nullptr;
+  MLFMA_CUDA(cudaStreamEndCapture(s, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  MLFMA_CUDA(e);
+  P.graphs.push_back(ApplyGraph{x, w, s, precision, exec});
+  MLFMA_CUDA(cudaGraphLaunch(exec, s));
+}
+
+void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
+  apply_graphed(P, x, w, s, 0, [&] { apply_direct(P, x, w, s); });
+}
+
+void clear_graphs(Plan& P) {
+  for (auto& g : P.graphs) cudaGraphExecDestroy(g.exec);
+  P.graphs.clear();
+}
+
 void apply_mixed_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   if (P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
-  apply_fixed<float2>(P, x, w, s);
+  apply_graphed(P, x, w, s, 1, [&] { apply_fixed<float2>(P, x, w, s); });
 }
 
 void apply_batch_mixed_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw,

@@ -19,9 +19,11 @@ Plan::~Plan() {
   if (device >= 0) {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     for (auto& set : prof.sets)
       for (cudaEvent_t e : set) cudaEventDestroy(e);
     for (void* p : allocations) cudaFree(p);
+    if (h_status) cudaFreeHost(h_status);
     if (stream) cudaStreamDestroy(stream);
     if (stream2) {
       cudaStreamSynchronize(stream2);
@@ -29,6 +31,12 @@ Plan::~Plan() {
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (stream_near) {
+      cudaStreamSynchronize(stream_near);
+      cudaStreamDestroy(stream_near);
+    }
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_near) cudaEventDestroy(ev_near);
     for (int m = 0; m < 2; ++m) {
       if (stream_leaf[m]) {
         cudaStreamSynchronize(stream_leaf[m]);
@@ -149,6 +157,9 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   MLFMA_CUDA(cudaStreamCreateWithFlags(&P->stream2, cudaStreamNonBlocking));
   MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
   MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
+  MLFMA_CUDA(cudaStreamCreateWithFlags(&P->stream_near, cudaStreamNonBlocking));
+  MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_start, cudaEventDisableTiming));
+  MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_near, cudaEventDisableTiming));
   for (int m = 0; m < 2; ++m) {
     MLFMA_CUDA(cudaStreamCreateWithFlags(&P->stream_leaf[m], cudaStreamNonBlocking));
     MLFMA_CUDA(cudaEventCreateWithFlags(&P->ev_agg[m], cudaEventDisableTiming));
@@ -404,6 +415,41 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
           P->lv[l].pair_ptr = P->upload(pptr);
           P->lv[l].pair_src = P->upload(psrc);
           P->lv[l].pair_vec = P->upload(pvec);
+          // merged lists of box groups (8q .. 8q+7)
+          const int G8 = (B + 7) / 8;
+          std::vector<int> gptr(G8 + 1, 0), gsrc;
+          std::vector<int4> gcode;
+          for (int q = 0; q < G8; ++q) {
+            const int nb = std::min(8, B - 8 * q);
+            int cur[8], end[8];
+            for (int j = 0; j < nb; ++j) {
+              cur[j] = Lv.far_ptr[8 * q + j];
+              end[j] = Lv.far_ptr[8 * q + j + 1];
+              for (int e = cur[j] + 1; e < end[j]; ++e)
+                if (Lv.far_idx[e] <= Lv.far_idx[e - 1]) throw std::runtime_error("interaction list not ascending");
+            }
+            for (;;) {
+              int src = INT32_MAX;
+              for (int j = 0; j < nb; ++j)
+                if (cur[j] < end[j]) src = std::min(src, Lv.far_idx[cur[j]]);
+              if (src == INT32_MAX) break;
+              unsigned w[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
+              for (int j = 0; j < nb; ++j)
+                if (cur[j] < end[j] && Lv.far_idx[cur[j]] == src) {
+                  const int code = fv[cur[j]++];
+                  if (code < 0 || code > 32767) throw std::runtime_error("transfer-factor row out of 16-bit range");
+                  const int sh = 16 * (j & 1);
+                  w[j >> 1] = (w[j >> 1] & ~(0xffffu << sh)) | (static_cast<unsigned>(code) << sh);
+                }
+              gsrc.push_back(src);
+              gcode.push_back(make_int4(static_cast<int>(w[0]), static_cast<int>(w[1]), static_cast<int>(w[2]),
+                                        static_cast<int>(w[3])));
+            }
+            gptr[q + 1] = static_cast<int>(gsrc.size());
+          }
+          P->lv[l].grp_ptr = P->upload(gptr);
+          P->lv[l].grp_src = P->upload(gsrc);
+          P->lv[l].grp_code = P->upload(gcode);
         }
         std::vector<double> rhat;
         std::vector<int> hoff, hL;
@@ -439,6 +485,10 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   }
   P->d_x = P->alloc<double2>(2 * static_cast<size_t>(P->N));
   P->d_w = P->alloc<double2>(2 * static_cast<size_t>(P->N));
+  P->d_status = P->alloc<int>(1);
+  MLFMA_CUDA(cudaMemsetAsync(P->d_status, 0, sizeof(int), s));
+  MLFMA_CUDA(cudaHostAlloc(&P->h_status, sizeof(int), cudaHostAllocDefault));
+  *P->h_status = 0;
   // complex64 copies of the operator's tables and its workspaces
   if (P->precision == 1) {
     auto copy32 = [&](const double2* src, size_t n) {

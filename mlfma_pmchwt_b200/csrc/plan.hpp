@@ -92,6 +92,13 @@ struct DevLevel {
   int* pair_ptr = nullptr;     // [ceil(B/2) + 1]
   int* pair_src = nullptr;
   int2* pair_vec = nullptr;
+  // boxes in groups of 8 (8q .. 8q+7): the merged, source-ordered union of
+  // the group's interaction lists; per entry the transfer-factor row of each
+  // member as 16-bit fields (member j in word j/2, bits 16*(j%2); -1: not
+  // in its list)
+  int* grp_ptr = nullptr;      // [ceil(B/8) + 1]
+  int* grp_src = nullptr;
+  int4* grp_code = nullptr;
   long long far_pairs = 0;
   int* coord = nullptr;        // [3 * B] integer box coordinates
   int* usrc_ptr = nullptr;     // per parent box (level - 1): union of its children's
@@ -107,18 +114,35 @@ struct DevLevel {
 
 // Kernel choices a plan can be tuned with (mlfma_set_tuning).
 struct Tuning {
-  int m2l_variant = 2;         // 0: one thread per (box, direction); 1: sibling-group tiles;
+  int m2l_variant = 4;         // 0: one thread per (box, direction); 1: sibling-group tiles;
                                // 2: octant registers over the sibling union, all levels per launch;
                                // 3: warp per box, 8 Morton-consecutive boxes per CTA, all levels per launch;
                                // 4: warp per box pair (merged lists), 4 pairs per CTA, all levels per launch;
-                               // 5: as 4 with the J and M halves on separate warps
+                               // 5: as 4 with the J and M halves on separate warps;
+                               // 6: groups of 8 boxes, the union's source patterns staged in shared
+                               //    memory by bulk asynchronous copies, 2 boxes per warp;
+                               // 7: as 6 with 4 boxes per warp
   int l2l_variant = 1;         // 0: 2-D transposed taps per child direction; 1: separable
-  int up_variant = 1;          // 0: 9-tap gather per parent direction; 1: separable in bands;
+  int up_variant = 0;          // 0: 9-tap gather per parent direction; 1: separable in bands;
                                // 2: 9-tap gather, all 6 components per thread;
                                // 3: separable in registers, 4-row bands per thread
-  int agg_variant = 1;         // 0: thread per (box, direction); 1: CTA per (box, medium) streaming
+  int agg_variant = 0;         // 0: thread per (box, direction); 1: CTA per (box, medium) streaming
                                //    the box's contiguous pattern block
+  int leaf_variant = 0;        // 0: near field inside the leaf kernel; 1: near field on its own
+                               //    stream from the start of the apply, the leaf kernel adds the far field
+  int graph = 1;               // 1: capture each apply (per x, w, stream and precision) as a CUDA
+                               //    graph on first use and replay it; 0: launch the kernels directly
 };
+
+// Captured applies, replayed when the same (x, w, stream, precision) recurs.
+struct ApplyGraph {
+  const void* x;
+  void* w;
+  cudaStream_t s;
+  int precision;
+  cudaGraphExec_t exec;
+};
+constexpr size_t kMaxApplyGraphs = 128;
 
 // Per-apply CUDA events between stage groups, recorded on the launching
 // stream: [m1 agg | m1 up | m1 m2l | m1 l2l | m2 agg | m2 up | m2 m2l | m2 l2l | leaf_out].
@@ -180,6 +204,8 @@ struct Plan {
   float2* d_near_z32 = nullptr;     // complex64 copy (precision = mixed)
   long long near_pairs = 0;
   // ---- vectors
+  int* d_status = nullptr;          // device status bits (a bounded wait that ran out)
+  int* h_status = nullptr;          // pinned host copy, read back by the host-pointer apply
   double2* d_x = nullptr;           // staging for host-pointer apply
   double2* d_w = nullptr;
   // ---- batched apply: leaf-level S / B arrays of each right-hand-side slot
@@ -199,7 +225,11 @@ struct Plan {
   // ev_agg[m] (aggregation done); ev_leaf[m] marks its end
   cudaStream_t stream_leaf[2] = {nullptr, nullptr};
   cudaEvent_t ev_agg[2] = {nullptr, nullptr}, ev_leaf[2] = {nullptr, nullptr};
+  // the near-field product runs on stream_near from ev_start to ev_near
+  cudaStream_t stream_near = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_near = nullptr;
   StageProfiler prof;
+  std::vector<ApplyGraph> graphs;
   size_t bytes = 0;
   std::vector<void*> allocations;
 
@@ -290,6 +320,7 @@ void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& 
                      const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s);
 void launch_near(Plan& P, cudaStream_t s);
 void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s);
+void clear_graphs(Plan& P);  // after any change that alters what an apply launches
 // Batched apply: W[j] = A X[j] for j < R; X[j] at X + j * ldx (ldx >= 2N),
 // the same for W. Right-hand sides go through in groups of kBatchSlots.
 constexpr int kBatchSlots = 16;

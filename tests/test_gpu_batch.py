@@ -91,3 +91,28 @@ def test_lockstep_solve_more_systems_than_slots(case_files):
     W = op.apply_batch(X)
     for j in range(19):
         assert rel(W[j], B[j]) < 1e-5 * 1.01
+
+
+def test_graph_replay_tracks_new_inputs(case_files):
+    """The captured apply is replayed for recurring pointers; each replay
+    reads the buffers' current contents (host path: the plan's own device
+    vectors; device path: the caller's pointers and stream)."""
+    import torch
+    from mlfma_pmchwt_b200 import mesh as M
+    op = gpu_op(case_files, "sphere_s3_lossy")
+    xs = [M.unit_disk_vector(op.n, 40 + j) for j in range(3)]
+    op.set_tuning("apply.graph", 0)
+    direct = [op.apply_ax(x) for x in xs]
+    op.set_tuning("apply.graph", 1)
+    for _ in range(2):
+        for x, w in zip(xs, direct):
+            assert rel(op.apply_ax(x), w) < 1e-14
+    stream = torch.cuda.Stream()
+    xd = torch.empty(op.n, dtype=torch.complex128, device="cuda")
+    wd = torch.empty_like(xd)
+    for x, w in zip(xs + xs, direct + direct):
+        xd.copy_(torch.from_numpy(x))
+        torch.cuda.synchronize()
+        op.apply_device(xd.data_ptr(), wd.data_ptr(), stream.cuda_stream)
+        stream.synchronize()
+        assert rel(wd.cpu().numpy(), w) < 1e-14
