@@ -172,6 +172,34 @@ def stage_bytes(op) -> dict:
     return b
 
 
+def translation_flops(op) -> float:
+    """FP64 flops of the translation per apply: every interaction-list pair,
+    both media, 6 pattern components, one complex multiply-add (8 flops)
+    per direction."""
+    inf = op.info
+    return float(sum(inf.far_pairs[i] * (inf.K_k1[i] + inf.K_k2[i]) * 6 * 8 for i in range(op.max_level - 1)))
+
+
+def fp64_peak_tflops(dev) -> float:
+    """Measured FP64 throughput of this GPU: cuBLAS DGEMM (torch.matmul on
+    float64, 4096^3), best of 5 with CUDA events."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        a @ b
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1))
+    return 2.0 * n ** 3 / (best / 1000.0) / 1e12
+
+
 def cpu_baseline_reference(args, wl, rank: int) -> dict | None:
     """The reference's own OpenMP matvec (oracle/_ref) on this host's cores."""
     from oracle import oracle as O
@@ -284,20 +312,20 @@ def multi_rhs_study(args, local: int) -> dict:
         its = [s_["iterations"] for s_ in st]
         return {"s_total": round(secs, 3), "s_per_rhs": round(secs / R, 4), "converged": sum(s_["converged"] for s_ in st),
                 "iterations_mean": round(float(np.mean(its)), 2), "iterations_max": int(max(its)),
-                "rel_residual_max": max(s_["rel_residual"] for s_ in st)}
+                "rel_residual_max": max(s_["rel_residual"] for s_ in st), "inner_its": args.study_inner_its}
 
     t = time.perf_counter()
-    Xm, sm = op.solve_mixed_batch(B, itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.inner_its)
+    Xm, sm = op.solve_mixed_batch(B, itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.study_inner_its)
     out["mixed_lockstep"] = record(sm, time.perf_counter() - t)
     out["mixed_lockstep"]["solver"] = ("lockstep FGMRES(50) with the complex64 operator and near-field "
                                        "preconditioner, FP64 refinement")
     t = time.perf_counter()
-    Xd, sd = op.matrix_solver_batch(B, itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.inner_its)
+    Xd, sd = op.matrix_solver_batch(B, itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.study_inner_its)
     out["fp64_lockstep"] = record(sd, time.perf_counter() - t)
     t = time.perf_counter()
-    x1, s1 = op.matrix_solver(B[0], itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.inner_its)
+    x1, s1 = op.matrix_solver(B[0], itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.study_inner_its)
     out["fp64_one_at_a_time_s_per_rhs"] = round(time.perf_counter() - t, 4)
-    Xo, so = op.matrix_solver_batch(B, itr_max=1000, mr=50, tol_abs=0.0, tol_rel=1e-6, inner_its=args.inner_its)
+    Xo, so = op.matrix_solver_batch(B, itr_max=1000, mr=50, tol_abs=0.0, tol_rel=1e-6, inner_its=args.study_inner_its)
     mono = lambda X: np.array([op.calculate_rcs_pmchwt(X[i], th[i], 0.0)[1][0, 0] for i in range(R)])
     ro = mono(Xo)
     dm, dd = np.abs(mono(Xm) - ro), np.abs(mono(Xd) - ro)
@@ -325,7 +353,7 @@ def bodies_study(args, local: int) -> dict:
         setup = time.perf_counter() - t0
         B = np.stack([op.compute_v_pmchwt(*plane_wave(90.0 * (i % 2), 12.0 * i, 0.0)) for i in range(16)])
         t1 = time.perf_counter()
-        X, st = op.solve_mixed_batch(B, itr_max=600, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.inner_its)
+        X, st = op.solve_mixed_batch(B, itr_max=600, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.study_inner_its)
         solve = time.perf_counter() - t1
         rows.append({"kind": b["kind"], "unknowns": op.n, "eps_r": [round(b["eps_r"].real, 3), round(b["eps_r"].imag, 4)],
                      "setup_s": round(setup, 3), "solve_s": round(solve, 3), "converged": sum(s_["converged"] for s_ in st),
@@ -435,7 +463,16 @@ def run_product(args):
                 "stage_note": "stage times from a pass with the two media one after the other; "
                               "the timed apply runs the media's tree passes on two streams",
                 "matvec_bytes": sum(sb.values()),
-                "matvec_frac": round(sum(sb.values()) / (ms_per_step / 1000.0) / 1e9 / peak, 4)}
+                "matvec_frac": round(sum(sb.values()) / (ms_per_step / 1000.0) / 1e9 / peak, 4),
+                "stage_hbm_frac": {k: round(sb[k] / (v / 1000.0) / 1e9 / peak, 4)
+                                   for k, v in per_apply_ms.items() if v > 0}}
+    # the translation is FP64-arithmetic- and L2-bound rather than HBM-bound:
+    # its second bound, against the measured DGEMM rate of this GPU
+    fp64_peak = fp64_peak_tflops(dev)
+    tflops = translation_flops(op) / (per_apply_ms["translation"] / 1000.0) / 1e12
+    roofline["fp64"] = {"kernel": "translation", "flops": translation_flops(op), "achieved": round(tflops, 2),
+                        "peak": round(fp64_peak, 2), "unit": "TFLOP/s", "frac": round(tflops / fp64_peak, 4),
+                        "peak_source": "measured in this run: cuBLAS DGEMM (torch float64 matmul 4096^3)"}
 
     # the complex64 operator of the same plan (mixed precision), same timing
     mixed = None
@@ -536,7 +573,9 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["product", "reference"], default="product")
     ap.add_argument("--size", choices=["full", "mid", "small"], default="full")
     ap.add_argument("--solve-its", type=int, default=300, help="outer iteration cap of the solves")
-    ap.add_argument("--inner-its", type=int, default=16, help="near-field GMRES steps per preconditioning")
+    ap.add_argument("--inner-its", type=int, default=None,
+                    help="near-field GMRES steps per preconditioning (default: 16 for the 245,760-unknown solve "
+                         "and the lockstep studies, 8 for single solves of the smaller spheres)")
     ap.add_argument("--plain-its", type=int, default=300, help="iteration cap of the plain GMRES comparison")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference matvecs to time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -547,6 +586,10 @@ def main(argv=None):
     ap.add_argument("--tuning", default="auto",
                     help="'auto' (autotune) or fixed kernel variants, e.g. m2l.variant=2,up.variant=1")
     args = ap.parse_args(argv)
+    # the lockstep studies (61,440-unknown sphere, 24 bodies) use 16 unless given
+    args.study_inner_its = 16 if args.inner_its is None else args.inner_its
+    if args.inner_its is None:
+        args.inner_its = 16 if args.size == "full" else 8
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_product(args)

@@ -185,11 +185,13 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  *                  1 = the near-field product on its own stream from the start
  *                  of the apply (it needs only x), overlapping the tree
  *                  passes; the leaf kernel then adds the far field.
- *   "apply.graph"  1 = each apply (per x, w, stream and precision) is captured
- *                  as a CUDA graph on first use and replayed afterwards
- *                  (default); 0 = direct launches. Setting any key drops the
- *                  captured graphs. The first apply with given pointers should
- *                  come before the caller captures its own graph.
+ *   "apply.graph"  1 = the apply of each (stream, precision) is captured as a
+ *                  CUDA graph on first use and replayed afterwards (default);
+ *                  the graph works on plan-owned vectors, x is copied in and
+ *                  w out around each replay (device copies of 2N values), so
+ *                  any x, w pair reuses it; 0 = direct launches. Setting any
+ *                  key drops the captured graphs. Inside a caller's own
+ *                  capture the apply launches directly.
  * mlfma_autotune times the values of each key in that order (the others held
  * at their current values) over `applies` applies of the plan's own operator
  * (device vectors owned by the plan) and keeps the fastest; variant_ms (may be

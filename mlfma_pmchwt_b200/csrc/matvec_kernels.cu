@@ -1906,41 +1906,52 @@ void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2
   }
 }
 
-// Replays the captured apply for (x, w, s, precision), capturing it on first
-// use; launches directly while stage profiling, inside another capture, or
-// when the cache is full. Returns false when the caller should launch directly.
+// Replays the captured apply of (stream, precision), capturing it on first
+// use. The graph reads and writes the plan's staging vectors d_gx / d_gw, so
+// that one graph serves every (x, w) pair: x is copied in and w out around
+// the replay (two device copies of 2N complex values, microseconds against
+// the apply), and a solver whose Krylov vectors change every iteration does
+// not capture a graph per vector. Launches directly while stage profiling,
+// inside another capture, or on the legacy default stream.
 template <class F>
 void apply_graphed(Plan& P, const double2* x, double2* w, cudaStream_t s, int precision, F&& launch) {
-  if (!P.tuning.graph || P.prof.on) return launch();
-  for (const ApplyGraph& g : P.graphs)
-    if (g.x == x && g.w == w && g.s == s && g.precision == precision) {
-      MLFMA_CUDA(cudaGraphLaunch(g.exec, s));
-      return;
-    }
+  if (!P.tuning.graph || P.prof.on || s == nullptr) return launch(x, w);
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   MLFMA_CUDA(cudaStreamIsCapturing(s, &cs));
-  if (cs != cudaStreamCaptureStatusNone || P.graphs.size() >= kMaxApplyGraphs || s == nullptr) return launch();
-  MLFMA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  try {
-    launch();
-  } catch (...) {
-    cudaGraph_t g = nullptr;
-    cudaStreamEndCapture(s, &g);
-    if (g) cudaGraphDestroy(g);
-    throw;
+  if (cs != cudaStreamCaptureStatusNone) return launch(x, w);
+  const size_t bytes = 2 * static_cast<size_t>(P.N) * sizeof(double2);
+  if (P.d_gx == nullptr) {
+    P.d_gx = P.alloc<double2>(2 * static_cast<size_t>(P.N));
+    P.d_gw = P.alloc<double2>(2 * static_cast<size_t>(P.N));
   }
-  cudaGraph_t graph = nullptr;
-  MLFMA_CUDA(cudaStreamEndCapture(s, &graph));
   cudaGraphExec_t exec = nullptr;
-  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-  cudaGraphDestroy(graph);
-  MLFMA_CUDA(e);
-  P.graphs.push_back(ApplyGraph{x, w, s, precision, exec});
+  for (const ApplyGraph& g : P.graphs)
+    if (g.s == s && g.precision == precision) exec = g.exec;
+  if (exec == nullptr && P.graphs.size() >= kMaxApplyGraphs) return launch(x, w);
+  if (x != P.d_gx) MLFMA_CUDA(cudaMemcpyAsync(P.d_gx, x, bytes, cudaMemcpyDeviceToDevice, s));
+  if (exec == nullptr) {
+    MLFMA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      launch(P.d_gx, P.d_gw);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cudaGraph_t graph = nullptr;
+    MLFMA_CUDA(cudaStreamEndCapture(s, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    MLFMA_CUDA(e);
+    P.graphs.push_back(ApplyGraph{s, precision, exec});
+  }
   MLFMA_CUDA(cudaGraphLaunch(exec, s));
+  if (w != P.d_gw) MLFMA_CUDA(cudaMemcpyAsync(w, P.d_gw, bytes, cudaMemcpyDeviceToDevice, s));
 }
 
 void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
-  apply_graphed(P, x, w, s, 0, [&] { apply_direct(P, x, w, s); });
+  apply_graphed(P, x, w, s, 0, [&](const double2* xx, double2* ww) { apply_direct(P, xx, ww, s); });
 }
 
 void clear_graphs(Plan& P) {
@@ -1950,7 +1961,7 @@ void clear_graphs(Plan& P) {
 
 void apply_mixed_device(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   if (P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
-  apply_graphed(P, x, w, s, 1, [&] { apply_fixed<float2>(P, x, w, s); });
+  apply_graphed(P, x, w, s, 1, [&](const double2* xx, double2* ww) { apply_fixed<float2>(P, xx, ww, s); });
 }
 
 void apply_batch_mixed_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw,

@@ -136,13 +136,11 @@ struct Tuning {
 
 // Captured applies, replayed when the same (x, w, stream, precision) recurs.
 struct ApplyGraph {
-  const void* x;
-  void* w;
   cudaStream_t s;
   int precision;
   cudaGraphExec_t exec;
 };
-constexpr size_t kMaxApplyGraphs = 128;
+constexpr size_t kMaxApplyGraphs = 16;
 
 // Per-apply CUDA events between stage groups, recorded on the launching
 // stream: [m1 agg | m1 up | m1 m2l | m1 l2l | m2 agg | m2 up | m2 m2l | m2 l2l | leaf_out].
@@ -206,6 +204,8 @@ struct Plan {
   // ---- vectors
   int* d_status = nullptr;          // device status bits (a bounded wait that ran out)
   int* h_status = nullptr;          // pinned host copy, read back by the host-pointer apply
+  double2* d_gx = nullptr;          // input / output vectors of the captured apply graphs
+  double2* d_gw = nullptr;
   double2* d_x = nullptr;           // staging for host-pointer apply
   double2* d_w = nullptr;
   // ---- batched apply: leaf-level S / B arrays of each right-hand-side slot

@@ -94,9 +94,10 @@ def test_lockstep_solve_more_systems_than_slots(case_files):
 
 
 def test_graph_replay_tracks_new_inputs(case_files):
-    """The captured apply is replayed for recurring pointers; each replay
-    reads the buffers' current contents (host path: the plan's own device
-    vectors; device path: the caller's pointers and stream)."""
+    """One captured apply per stream serves every (x, w) pair: each replay
+    reads the current contents of the caller's x and writes the caller's w
+    (host path: the plan's own device vectors; device path: the caller's
+    pointers and stream, recurring and new ones)."""
     import torch
     from mlfma_pmchwt_b200 import mesh as M
     op = gpu_op(case_files, "sphere_s3_lossy")
@@ -116,3 +117,13 @@ def test_graph_replay_tracks_new_inputs(case_files):
         op.apply_device(xd.data_ptr(), wd.data_ptr(), stream.cuda_stream)
         stream.synchronize()
         assert rel(wd.cpu().numpy(), w) < 1e-14
+    # a new pair of device vectors per apply (as a Krylov basis gives)
+    X = [torch.from_numpy(x).to("cuda") for x in xs]
+    W = [torch.full_like(X[0], float("nan")) for _ in xs]
+    torch.cuda.synchronize()
+    for xj, wj in zip(X, W):
+        op.apply_device(xj.data_ptr(), wj.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    for wj, w in zip(W, direct):
+        assert rel(wj.cpu().numpy(), w) < 1e-14
+    assert op.device_status() == 0
