@@ -281,7 +281,8 @@ def parse_tuning(spec: str) -> dict | None:
 
 def solve_record(st: dict, inner_its: int) -> dict:
     rec = {"s_per_rhs": round(st["seconds"], 4), "iterations": st["iterations"], "converged": st["converged"],
-           "rel_residual": st["rel_residual"], "restart": 50, "tol": 1e-3, "matvecs": st["matvecs"]}
+           "rel_residual": st["rel_residual"], "restart": 50, "tol": 1e-3, "matvecs": st["matvecs"],
+           "timing": "faster of two identical solves"}
     if inner_its:
         rec["solver"] = f"FGMRES(50), right preconditioner = {inner_its} GMRES steps on the near field"
         rec["near_products"] = st["near_products"]
@@ -500,15 +501,22 @@ def run_product(args):
     # (2) the same with complex-argument transfer factors h2_l(k2 R), which
     # the lossy medium needs for the far field to match its near field.
     solve = None
+    def warm(fn):
+        """Runs an identical solve twice and keeps the faster (the first also
+        pays first-use costs such as the apply graph's capture)."""
+        a, b = fn(), fn()
+        return a if a[1]["seconds"] <= b[1]["seconds"] else b
+
     if args.solve_its > 0:
         from mlfma_pmchwt_b200 import plane_wave
         V = op.compute_v_pmchwt(*plane_wave(0.0, 0.0, 0.0))
-        _, st = op.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
-                                 inner_its=args.inner_its)
+        _, st = warm(lambda: op.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
+                                              inner_its=args.inner_its))
         solve = {"reference_transfer": solve_record(st, args.inner_its)}
         if args.plain_its > 0:
             _, sp_ = op.matrix_solver(V, itr_max=args.plain_its, mr=50, tol_abs=1e-8, tol_rel=1e-3)
             solve["reference_transfer_plain_gmres"] = solve_record(sp_, 0)
+            solve["reference_transfer_plain_gmres"]["timing"] = "one solve"
         if wl["eps"].imag != 0.0:
             op.close()
             opc = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local,
@@ -516,12 +524,12 @@ def run_product(args):
             for k, v in tune.items():
                 if not k.endswith("_ms"):
                     opc.set_tuning(k, v)
-            _, sc = opc.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
-                                      inner_its=args.inner_its)
+            _, sc = warm(lambda: opc.matrix_solver(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
+                                                   inner_its=args.inner_its))
             solve["complex_transfer"] = solve_record(sc, args.inner_its)
             if args.mixed:
-                _, sm = opc.solve_mixed(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
-                                        inner_its=args.inner_its, refine_max=10)
+                _, sm = warm(lambda: opc.solve_mixed(V, itr_max=args.solve_its, mr=50, tol_abs=1e-8, tol_rel=1e-3,
+                                                     inner_its=args.inner_its, refine_max=10))
                 rec = solve_record(sm, args.inner_its)
                 rec["solver"] = ("FP64 iterative refinement around complex64 " + rec["solver"] +
                                  "; residual checked with the FP64 operator")

@@ -218,7 +218,10 @@ MLFMA_API int mlfma_gmres(mlfma_plan* plan, int n, double* x, const double* rhs,
  * CGS (Code/CGS.h). Arguments, stopping rule, true residual per cycle and
  * divergence abort are those of mlfma_gmres. The right preconditioner is
  * inner_its GMRES steps from zero on the near-field matrix alone (the Z_near
- * rows of Code/Zmartix.h:541-643); inner_its = 0 reduces to plain GMRES.
+ * rows of Code/Zmartix.h:541-643), whose products use the plan's complex64
+ * copy of Z_near (a flexible outer iteration admits any preconditioner; the
+ * operator and the true residual stay FP64); inner_its = 0 reduces to plain
+ * GMRES.
  * itr_max counts outer steps; stats->near_products counts inner products. */
 MLFMA_API int mlfma_fgmres(mlfma_plan* plan, int n, double* x, const double* rhs, int itr_max, int mr,
                            double tol_abs, double tol_rel, int inner_its, mlfma_solve_stats* stats,

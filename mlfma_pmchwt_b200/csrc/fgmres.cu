@@ -87,7 +87,7 @@ void back_substitute(const std::vector<C>& H, int ld, const std::vector<C>& s, i
 
 void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s, int prec) {
   if (prec == 1) {
-    if (P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
+    if (P.d_near_z32 == nullptr) throw std::invalid_argument("plan holds no complex64 near field");
     NearArg<float2> a{P.d_leaf_rwg,  P.d_rwg_leafbox, P.d_leaf_ptr, P.d_near_sptr, P.d_near_src,
                       P.d_near_zoff, P.d_near_z32,    x,            w,             P.N};
     near_apply_kernel<float2><<<(P.N + 3) / 4, 128, 0, s>>>(a);
@@ -143,7 +143,10 @@ bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, d
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return ok;
   };
-  // z = approximate solution of Z_near z = v by inner_its GMRES steps from zero
+  // z = approximate solution of Z_near z = v by inner_its GMRES steps from
+  // zero, with the complex64 copy of Z_near (the outer flexible GMRES admits
+  // any preconditioner; its operator and residuals stay at the solve's
+  // precision)
   std::vector<C> Hi(static_cast<size_t>(inner_its + 1) * std::max(inner_its, 1)), ci(inner_its + 1),
       si(inner_its + 1), gi(inner_its + 1), yi;
   auto precondition = [&](const double2* v, double2* z) {
@@ -156,7 +159,7 @@ bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, d
     int used = 0;
     for (int j = 0; j < inner_its; ++j) {
       double2* u = Q + static_cast<long long>(j + 1) * n;
-      near_apply(P, Q + static_cast<long long>(j) * n, u, s, prec);
+      near_apply(P, Q + static_cast<long long>(j) * n, u, s, 1);
       st.near_products++;
       const double hn = ops.orthogonalise(Q, j + 1, u, hcol);
       for (int i = 0; i <= j; ++i) Hi[i + j * ld] = hcol[i];

@@ -422,18 +422,12 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
     std::vector<double> hn;
     for (int j = 0; j < inner_its; ++j) {
       const dim3 ng((P.N + 3) / 4, (Ra + kNearRB - 1) / kNearRB);
-      if (prec == 1) {
+      {  // the preconditioner's near field is the complex64 copy at either precision
         NearBatchArg<float2> na{P.d_leaf_rwg,  P.d_rwg_leafbox,      P.d_leaf_ptr,
                                 P.d_near_sptr, P.d_near_src,         P.d_near_zoff,
                                 P.d_near_z32,  sysref(Q, qs, j * n), sysref(Q, qs, (j + 1) * n),
                                 sysd,          P.N,                  Ra};
         near_batch_kernel<float2><<<ng, 128, 0, s>>>(na);
-      } else {
-        NearBatchArg<double2> na{P.d_leaf_rwg,  P.d_rwg_leafbox,      P.d_leaf_ptr,
-                                 P.d_near_sptr, P.d_near_src,         P.d_near_zoff,
-                                 P.d_near_z,    sysref(Q, qs, j * n), sysref(Q, qs, (j + 1) * n),
-                                 sysd,          P.N,                  Ra};
-        near_batch_kernel<double2><<<ng, 128, 0, s>>>(na);
       }
       MLFMA_CUDA(cudaGetLastError());
       for (int q : list) st[q].near_products++;

@@ -512,7 +512,13 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
         }
       }
     }
-    P->d_near_z32 = copy32(P->d_near_z, 3 * static_cast<size_t>(std::max<long long>(P->near_pairs, 1)));
+  }
+  // complex64 copy of the near field: the flexible GMRES preconditioner's
+  // products (any plan) and the mixed operator's near rows
+  {
+    const size_t nz = 3 * static_cast<size_t>(std::max<long long>(P->near_pairs, 1));
+    P->d_near_z32 = P->alloc<float2>(nz);
+    to_c64(P->d_near_z, P->d_near_z32, nz, s);
   }
   MLFMA_CUDA(cudaStreamSynchronize(s));
   P->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -199,7 +199,7 @@ struct Plan {
   int* d_near_src = nullptr;        // concatenated source RWG ids per box
   long long* d_near_zoff = nullptr; // [Bleaf+1]
   double2* d_near_z = nullptr;      // [pairs][3]
-  float2* d_near_z32 = nullptr;     // complex64 copy (precision = mixed)
+  float2* d_near_z32 = nullptr;     // complex64 copy: preconditioner products, mixed operator
   long long near_pairs = 0;
   // ---- vectors
   int* d_status = nullptr;          // device status bits (a bounded wait that ran out)
