@@ -959,19 +959,21 @@ __global__ void __launch_bounds__(32 * (kGrpBoxes / kBW + 1)) m2l_grp_kernel(con
     }
     const int4 cw = codes[st];
     const C* sp = stage + st * kGrpRows * kGrpDirs + lane;
-    int cc[kBW];
-    C t[kBW];
+    unsigned mask = 0;  // this warp's boxes that list the source (warp-uniform)
 #pragma unroll
-    for (int j = 0; j < kBW; ++j) {
-      cc[j] = grp_field(cw, warp * kBW + j);
-      t[j] = sp[(6 + warp * kBW + j) * kGrpDirs];  // not used when cc[j] < 0
-    }
+    for (int j = 0; j < kBW; ++j) mask |= (grp_field(cw, warp * kBW + j) >= 0 ? 1u : 0u) << j;
+    if (mask != 0) {
+      C sv[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      const C sv = sp[c * kGrpDirs];
+      for (int c = 0; c < 6; ++c) sv[c] = sp[c * kGrpDirs];
 #pragma unroll
-      for (int j = 0; j < kBW; ++j)
-        if (cc[j] >= 0) acc[j][c] = cfma(t[j], sv, acc[j][c]);
+      for (int j = 0; j < kBW; ++j) {
+        if (mask & (1u << j)) {
+          const C t = sp[(6 + warp * kBW + j) * kGrpDirs];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) acc[j][c] = cfma(t, sv[c], acc[j][c]);
+        }
+      }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(empty + st);
