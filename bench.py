@@ -342,12 +342,18 @@ def bodies_study(args, local: int) -> dict:
     ellipsoids, superellipsoids; 3,840-61,440 unknowns; lossy eps_r), 16
     plane waves each (theta_i = i * 180/15, phi = 0, polarisation alternating),
     solved to 1e-3 per body by lockstep FGMRES with the complex64 operator
-    inside FP64 refinement. Bodies go one after another, each with its own
-    plan; transfer factors with the complex argument (the bodies are lossy)."""
+    inside FP64 refinement; transfer factors with the complex argument (the
+    bodies are lossy). Each body has its own plan (and so its own streams);
+    --bodies-workers host threads run that many bodies at once, so that the
+    small bodies' launches and host round trips overlap on the GPU."""
+    from concurrent.futures import ThreadPoolExecutor
+
     from mlfma_pmchwt_b200 import MLFMM, plane_wave
     from mlfma_pmchwt_b200 import mesh as M
-    rows, t_all = [], time.perf_counter()
-    for b in M.uneven_bodies(1, FREQ):
+    import torch
+
+    def one(b):
+        torch.cuda.set_device(local)
         t0 = time.perf_counter()
         op = MLFMM(b["mesh"], freq=FREQ, eps_r=b["eps_r"], leaf_coeff=0.25, device=local, precision="mixed",
                    tf_complex_argument=True)
@@ -356,12 +362,19 @@ def bodies_study(args, local: int) -> dict:
         t1 = time.perf_counter()
         X, st = op.solve_mixed_batch(B, itr_max=600, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.study_inner_its)
         solve = time.perf_counter() - t1
-        rows.append({"kind": b["kind"], "unknowns": op.n, "eps_r": [round(b["eps_r"].real, 3), round(b["eps_r"].imag, 4)],
-                     "setup_s": round(setup, 3), "solve_s": round(solve, 3), "converged": sum(s_["converged"] for s_ in st),
-                     "iterations_mean": round(float(np.mean([s_["iterations"] for s_ in st])), 1)})
+        row = {"kind": b["kind"], "unknowns": op.n, "eps_r": [round(b["eps_r"].real, 3), round(b["eps_r"].imag, 4)],
+               "setup_s": round(setup, 3), "solve_s": round(solve, 3), "converged": sum(s_["converged"] for s_ in st),
+               "iterations_mean": round(float(np.mean([s_["iterations"] for s_ in st])), 1)}
         op.close()
+        return row
+
+    bodies = M.uneven_bodies(1, FREQ)
+    t_all = time.perf_counter()
+    workers = max(1, args.bodies_workers)
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        rows = list(pool.map(one, bodies))
     total = time.perf_counter() - t_all
-    return {"bodies": len(rows), "rhs": 16 * len(rows), "total_s": round(total, 2),
+    return {"bodies": len(rows), "rhs": 16 * len(rows), "workers": workers, "total_s": round(total, 2),
             "s_per_rhs": round(total / (16 * len(rows)), 4),
             "converged": sum(r["converged"] for r in rows), "per_body": rows}
 
@@ -591,6 +604,8 @@ def main(argv=None):
     ap.add_argument("--bodies", action="store_true", help="also run the 24-body uneven batch study")
     ap.add_argument("--no-mixed", dest="mixed", action="store_false",
                     help="skip the complex64 (mixed-precision) operator and solve")
+    ap.add_argument("--bodies-workers", type=int, default=4,
+                    help="bodies solved at once by the --bodies study (host threads, one plan each)")
     ap.add_argument("--tuning", default="auto",
                     help="'auto' (autotune) or fixed kernel variants, e.g. m2l.variant=2,up.variant=1")
     args = ap.parse_args(argv)
