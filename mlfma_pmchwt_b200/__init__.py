@@ -81,6 +81,7 @@ SIGNATURES = {
     "mlfma_device_status": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "mlfma_apply_batch": (C.c_int, [_P, C.c_int, C.c_int, _DP, _DP]),
     "mlfma_apply_batch_device": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P]),
+    "mlfma_apply_batch_mixed_device": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P]),
     "mlfma_profile": (C.c_int, [_P, C.c_int]),
     "mlfma_profile_read": (C.c_int, [_P, _DP, C.POINTER(C.c_int)]),
     "mlfma_set_tuning": (C.c_int, [_P, C.c_char_p, C.c_int]),
@@ -302,13 +303,19 @@ class MLFMM:
         self._check(self._lib.mlfma_apply_batch_device(self._h, self.n, int(R), C.c_void_p(x_ptr),
                                                        C.c_void_p(w_ptr), C.c_void_p(stream or 0)))
 
+    def apply_batch_mixed_device(self, R: int, x_ptr: int, w_ptr: int, stream: int | None = None):
+        """Batched apply with the complex64 operator on device pointers
+        (complex128 [R, 2N]; mixed-precision plans); asynchronous on `stream`."""
+        self._check(self._lib.mlfma_apply_batch_mixed_device(self._h, self.n, int(R), C.c_void_p(x_ptr),
+                                                             C.c_void_p(w_ptr), C.c_void_p(stream or 0)))
+
     def set_tuning(self, key: str, value: int):
         self._check(self._lib.mlfma_set_tuning(self._h, key.encode(), int(value)))
 
     def get_tuning(self, key: str) -> int:
         return self._check(self._lib.mlfma_get_tuning(self._h, key.encode()))
 
-    TUNING_KEYS = (("m2l.variant", 9), ("up.variant", 4), ("l2l.variant", 2), ("agg.variant", 2), ("leaf.variant", 2), ("apply.graph", 2))
+    TUNING_KEYS = (("m2l.variant", 9), ("up.variant", 4), ("l2l.variant", 2), ("agg.variant", 2), ("leaf.variant", 2), ("batch_agg.variant", 2), ("apply.graph", 2))
 
     def autotune(self, applies: int = 3) -> dict:
         """Times the values of each tuning key on this plan (one key at a

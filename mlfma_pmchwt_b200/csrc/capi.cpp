@@ -246,6 +246,23 @@ int mlfma_apply_batch_device(mlfma_plan* plan, int n, int R, const void* x_dev, 
   });
 }
 
+int mlfma_apply_batch_mixed_device(mlfma_plan* plan, int n, int R, const void* x_dev, void* w_dev, void* stream) {
+  if (!plan || !plan->p || !x_dev || !w_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (R <= 0) return fail(MLFMA_ERR_ARG, "R must be positive");
+  if (x_dev == w_dev) return fail(MLFMA_ERR_ARG, "x and w must not alias");
+  if (!device_plan(plan) || plan->p->precision != 1)
+    return fail(MLFMA_ERR_UNSUPPORTED, "plan was not created with MLFMA_PREC_MIXED on a device");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    mlfma::reserve_batch(P, R);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::apply_batch_mixed_device(P, R, static_cast<const double2*>(x_dev), n, static_cast<double2*>(w_dev), n, s);
+    return MLFMA_OK;
+  });
+}
+
 int mlfma_profile(mlfma_plan* plan, int on) {
   if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
   if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
@@ -277,6 +294,7 @@ constexpr TuningKey kTuningKeys[] = {
     {"l2l.variant", &mlfma::Tuning::l2l_variant, 2},
     {"agg.variant", &mlfma::Tuning::agg_variant, 2},
     {"leaf.variant", &mlfma::Tuning::leaf_variant, 2},
+    {"batch_agg.variant", &mlfma::Tuning::batch_agg, 2},
     {"apply.graph", &mlfma::Tuning::graph, 2},
 };
 const TuningKey* find_key(const char* key) {
@@ -330,6 +348,12 @@ int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
     // one key at a time, the others held at their current (best so far) value
     int slot = 0;
     for (const TuningKey& k : kTuningKeys) {
+      if (k.field == &mlfma::Tuning::batch_agg) {  // no effect on the single apply timed here
+        if (variant_ms)
+          for (int v = 0; v < k.count; ++v) variant_ms[slot + v] = -1.0;
+        slot += k.count;
+        continue;
+      }
       double best = 1e300;
       int best_v = P.tuning.*(k.field);
       for (int v = 0; v < k.count; ++v) {

@@ -23,6 +23,7 @@
 #include <type_traits>
 #include <utility>
 
+#include "agg_tc.hpp"
 #include "bulk.cuh"
 #include "cplx.cuh"
 #include "plan.hpp"
@@ -1740,7 +1741,29 @@ void apply_batch_fixed(Plan& P, int R, const double2* X, long long ldx, double2*
     ag.ldx = ldx;
     ag.N = P.N;
     ag.R = rn;
-    agg_batch_kernel<C, kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
+    bool on_tensor_cores = false;
+    if constexpr (std::is_same<C, float2>::value) {
+      if (P.tuning.batch_agg == 1 && agg_tc_supported(P, rn)) {
+        AggTcArg t{};
+        for (int m = 0; m < 2; ++m) {
+          t.Vs[m] = reinterpret_cast<const float*>(ag.Vs[m]);
+          t.K[m] = ag.K[m];
+          for (int j = 0; j < rn; ++j) t.S[m][j] = ag.S[m][j];
+        }
+        t.leaf_ptr = ag.leaf_ptr;
+        t.leaf_rwg = ag.leaf_rwg;
+        t.X = ag.X;
+        t.ldx = ag.ldx;
+        t.N = ag.N;
+        t.R = rn;
+        t.kmax = (P.max_leaf_rwgs + 7) & ~7;
+        t.status = P.d_status;
+        launch_agg_tc(P, t, s);
+        on_tensor_cores = true;
+      }
+    }
+    if (!on_tensor_cores)
+      agg_batch_kernel<C, kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
     {
       MediumStreams ms(P, s, true);
       for (int j = 0; j < rn; ++j)

@@ -464,6 +464,9 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   {
     const Level& Lf = T.lv[L];
     P->d_leaf_ptr = P->upload(T.leaf_ptr);
+    P->max_leaf_rwgs = 0;
+    for (size_t b = 0; b + 1 < T.leaf_ptr.size(); ++b)
+      P->max_leaf_rwgs = std::max(P->max_leaf_rwgs, T.leaf_ptr[b + 1] - T.leaf_ptr[b]);
     P->d_leaf_rwg = P->upload(T.leaf_rwg);
     P->d_rwg_leafbox = P->upload(T.rwg_leaf);
     P->d_leaf_center = P->upload(Lf.center);

@@ -128,6 +128,8 @@ struct Tuning {
                                // 3: separable in registers, 4-row bands per thread
   int agg_variant = 0;         // 0: thread per (box, direction); 1: CTA per (box, medium) streaming
                                //    the box's contiguous pattern block
+  int batch_agg = 1;           // batched complex64 aggregation: 0 CUDA cores; 1 tcgen05 tensor cores
+                               //    (3xTF32 split, TMEM accumulators)
   int leaf_variant = 0;        // 0: near field inside the leaf kernel; 1: near field on its own
                                //    stream from the start of the apply, the leaf kernel adds the far field
   int graph = 1;               // 1: capture each apply (per x, w, stream and precision) as a CUDA
@@ -184,6 +186,7 @@ struct Plan {
   double* d_quad = nullptr;         // [4][nq]: l1, l2, l3, w
   // ---- leaf data
   int* d_leaf_ptr = nullptr;        // [Bleaf+1] into leaf order
+  int max_leaf_rwgs = 0;            // most RWGs in one leaf box
   int* d_leaf_rwg = nullptr;        // leaf order -> RWG id
   int* d_rwg_leafbox = nullptr;     // [N] leaf box of each RWG id
   double* d_leaf_center = nullptr;  // [3 * Bleaf]
