@@ -147,10 +147,10 @@ MLFMA_API int mlfma_device_status(mlfma_plan* plan, int* status);
 MLFMA_API int mlfma_apply_batch(mlfma_plan* plan, int n, int R, const double* x, double* w);
 /* The batched apply with the complex64 operator (a plan created with
  * MLFMA_PREC_MIXED), device vectors as in mlfma_apply_batch_device. Its leaf
- * aggregation runs on the tensor cores (tcgen05, TF32 operands split into high
- * and low parts, FP32 accumulation in TMEM) when the tuning key
- * "batch_agg.variant" is 1 and every leaf box holds at most 64 RWGs, else on
- * the CUDA cores. No counterpart in the reference. */
+ * aggregation and far-field testing run on the tensor cores (tcgen05, TF32
+ * operands split into high and low parts, FP32 accumulation in TMEM) when the
+ * tuning key "batch_tc.variant" is 1 and every leaf box holds at most 64 RWGs,
+ * else on the CUDA cores. No counterpart in the reference. */
 MLFMA_API int mlfma_apply_batch_mixed_device(mlfma_plan* plan, int n, int R, const void* x_dev, void* w_dev,
                                              void* stream);
 MLFMA_API int mlfma_apply_batch_device(mlfma_plan* plan, int n, int R, const void* x_dev, void* w_dev,
@@ -189,10 +189,10 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  *   "agg.variant"  aggregation: 0 = one thread per (leaf box, direction), one
  *                  launch per medium (default); 1 = one CTA per (leaf box,
  *                  medium) streaming the box's contiguous pattern block.
- *   "batch_agg.variant" (the batched complex64 apply only) 0 = leaf aggregation
- *                  on the CUDA cores; 1 = on the tensor cores (tcgen05
- *                  kind::tf32 with high/low operand splitting, boxes of at
- *                  most 64 RWGs; default).
+ *   "batch_tc.variant" (the batched complex64 apply only) 0 = leaf aggregation
+ *                  and far-field testing on the CUDA cores; 1 = on the tensor
+ *                  cores (tcgen05 kind::tf32 with high/low operand splitting,
+ *                  boxes of at most 64 RWGs; default).
  *   "leaf.variant" 0 = the near-field rows inside the leaf testing kernel (default);
  *                  1 = the near-field product on its own stream from the start
  *                  of the apply (it needs only x), overlapping the tree
@@ -208,8 +208,8 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  * at their current values) over `applies` applies of the plan's own operator
  * (device vectors owned by the plan) and keeps the fastest; variant_ms (may be
  * NULL) receives the per-apply ms of every value, keys in that order
- * (23 entries: m2l 0-8, up 0-3, l2l 0-1, agg 0-1, leaf 0-1, batch_agg 0-1, graph 0-1).
- * "batch_agg.variant" acts on the batched complex64 apply only: autotune
+ * (23 entries: m2l 0-8, up 0-3, l2l 0-1, agg 0-1, leaf 0-1, batch_tc 0-1, graph 0-1).
+ * "batch_tc.variant" acts on the batched complex64 apply only: autotune
  * leaves it as set and reports -1 for its entries. */
 MLFMA_API int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value);
 MLFMA_API int mlfma_get_tuning(const mlfma_plan* plan, const char* key);

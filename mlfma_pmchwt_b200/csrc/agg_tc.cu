@@ -32,6 +32,7 @@
 
 #include "agg_tc.hpp"
 #include "bulk.cuh"
+#include "cplx.cuh"
 #include "plan.hpp"
 
 namespace mlfma {
@@ -65,7 +66,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 
 // Instruction descriptor, kind::tf32: FP32 accumulator, TF32 A and B, both
 // K-major, N >> 3 at bit 17, M >> 4 at bit 24.
-constexpr uint32_t idesc_tf32(int M, int N) {
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
          (static_cast<uint32_t>(M >> 4) << 24);
 }
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(128, 1) agg_tc_kernel(const __grid_constant__ 
   uint32_t* Blo = Bhi + kTcCols * a.kmax;
   uint64_t* bar = reinterpret_cast<uint64_t*>(Blo + kTcCols * a.kmax);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  int* sid = reinterpret_cast<int*>(tslot + 2);  // RWG ids of the box, [kmax]
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
@@ -116,19 +118,26 @@ __global__ void __launch_bounds__(128, 1) agg_tc_kernel(const __grid_constant__ 
     mbar_init(bar, 1);
     mbar_init_fence();
   }
-  // B: the box's currents, real column n = 2 * (part * R + j) + (0 re, 1 im)
-  for (int i = tid; i < kTcCols * kp; i += blockDim.x) {
-    const int n = i % kTcCols, k = i / kTcCols;
-    float v = 0.f;
-    if (k < nb && n < 4 * R) {
-      const int col = n >> 1, part = col / R, j = col - part * R;
-      const double2 x = a.X[j * a.ldx + part * a.N + a.leaf_rwg[r0 + k]];
-      v = static_cast<float>((n & 1) ? x.y : x.x);
+  for (int k = tid; k < nb; k += blockDim.x) sid[k] = a.leaf_rwg[r0 + k];
+  __syncthreads();
+  // B: the box's currents, real column n = 2 * col + (0 re, 1 im) with
+  // col = part * R + j; one complex current per (k, col) and thread
+#pragma unroll 4
+  for (int i = tid; i < (kTcCols / 2) * kp; i += blockDim.x) {
+    const int col = i % (kTcCols / 2), k = i / (kTcCols / 2);
+    float vr = 0.f, vi = 0.f;
+    if (k < nb && col < 2 * R) {
+      const int part = col / R, j = col - part * R;
+      const double2 x = a.X[j * a.ldx + part * a.N + sid[k]];
+      vr = static_cast<float>(x.x);
+      vi = static_cast<float>(x.y);
     }
-    const uint32_t hi = tf32_rna(v), lo = tf32_rna(v - __uint_as_float(hi));
-    const uint32_t o = kmajor_offset(n, k, kTcCols) >> 2;
-    Bhi[o] = hi;
-    Blo[o] = lo;
+    const uint32_t hr = tf32_rna(vr), hi = tf32_rna(vi);
+    const uint32_t o = kmajor_offset(2 * col, k, kTcCols) >> 2, o1 = kmajor_offset(2 * col + 1, k, kTcCols) >> 2;
+    Bhi[o] = hr;
+    Blo[o] = tf32_rna(vr - __uint_as_float(hr));
+    Bhi[o1] = hi;
+    Blo[o1] = tf32_rna(vi - __uint_as_float(hi));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -141,12 +150,20 @@ __global__ void __launch_bounds__(128, 1) agg_tc_kernel(const __grid_constant__ 
   bool ok = true;
   for (int mt = 0; mt * kTcRows < M6 && ok; ++mt) {
     const int q = mt * kTcRows + tid;  // this thread's real row (A row, TMEM lane)
-    for (int k = 0; k < kp; ++k) {
-      const float v = (k < nb && q < M6) ? __ldg(V + static_cast<size_t>(k) * M6 + q) : 0.f;
-      const uint32_t hi = tf32_rna(v), lo = tf32_rna(v - __uint_as_float(hi));
-      const uint32_t o = kmajor_offset(tid, k, kTcRows) >> 2;
-      Ahi[o] = hi;
-      Alo[o] = lo;
+    for (int k0 = 0; k0 < kp; k0 += 8) {  // 8 loads in flight per thread
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = k0 + u;
+        v[u] = (k < nb && q < M6) ? __ldg(V + static_cast<size_t>(k) * M6 + q) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const uint32_t hi = tf32_rna(v[u]), lo = tf32_rna(v[u] - __uint_as_float(hi));
+        const uint32_t o = kmajor_offset(tid, k0 + u, kTcRows) >> 2;
+        Ahi[o] = hi;
+        Alo[o] = lo;
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic smem writes -> tensor-core reads
     __syncthreads();
@@ -206,10 +223,234 @@ __global__ void __launch_bounds__(128, 1) agg_tc_kernel(const __grid_constant__ 
   }
 }
 
+// Far-field testing (see LeafTcArg). One real GEMM per (box, 32-RWG tile,
+// medium): A rows 4 rr + t for RWG rr, t = 0 / 1 the real / imaginary row of
+// Vf and t = 2 / 3 those of W = (-khat) x Vf, over real K = 2 x 3K (entry e
+// gives columns 2e (re) and 2e + 1 (im)): a real row holds (a_re, -a_im), an
+// imaginary row (a_im, a_re), so that D[real row] and D[imaginary row] are
+// the real and imaginary parts of sum_e a_e b_e. B: column part * 16 + j is
+// Bm_j of the box (part 0 the J half, 1 the M half), whose interleaved
+// complex layout already is the real K order. The K extent streams through
+// two shared-memory stages of 16 entries (32 real) each: the MMAs of one
+// stage run while the threads fill the other.
+constexpr int kLfRows = 128;      // 32 RWGs x 4 rows
+constexpr int kLfCols = 32;       // 2 parts x 16 slots
+constexpr int kLfChunk = 16;      // complex entries per stage (32 real K)
+constexpr int kLfStageA = kLfRows * 2 * kLfChunk;  // tf32 values per A operand stage
+constexpr int kLfStageB = kLfCols * 2 * kLfChunk;
+
+__global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__ LeafTcArg a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int b = blockIdx.x, tile = blockIdx.y;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int rb0 = a.leaf_ptr[b], nb = a.leaf_ptr[b + 1] - rb0;
+  const int rt0 = tile * 32;
+  if (rt0 >= nb) return;
+  const int nt = min(32, nb - rt0);  // RWGs of this tile
+  // stage s: A high, A low, B high, B low
+  uint32_t* const stage0 = reinterpret_cast<uint32_t*>(smem);
+  constexpr int kStage = 2 * (kLfStageA + kLfStageB);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * 2 * (kLfStageA + kLfStageB) * sizeof(uint32_t));
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                 "r"(2 * kLfCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+    mbar_init_fence();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  constexpr uint32_t idesc = idesc_tf32(kLfRows, kLfCols);
+  const int R = a.R;
+  const int rr = lane >> 2, t = lane & 3;  // epilogue: RWG (of this warp's 8) and row kind of this lane
+  float2 wj[4], wm[4];                     // slots j = 4 jj + t of RWG 8 warp + rr
+#pragma unroll
+  for (int q = 0; q < 4; ++q) wj[q] = wm[q] = make_float2(0.f, 0.f);
+  // Each chunk's MMAs start a fresh accumulator (TMEM columns 32 x stage);
+  // its 32 columns are added into dacc (FP32, round to nearest) when the
+  // stage comes round again or the medium ends, so that the tensor cores
+  // never accumulate more than one chunk (12 MMAs) in place.
+  const uint32_t lane_base = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+  float dacc[kLfCols];
+  auto drain = [&](int stage) {
+    float d[kLfCols];
+    tmem_ld16(lane_base + stage * kLfCols, d);
+    tmem_ld16(lane_base + stage * kLfCols + 16, d + 16);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int n = 0; n < kLfCols; ++n) dacc[n] += d[n];
+  };
+  int gc = 0;  // chunks issued so far (both media): stage gc & 1
+  bool ok = true;
+  for (int m = 0; m < 2 && ok; ++m) {
+    const int K = a.K[m], K3 = 3 * K;
+#pragma unroll
+    for (int n = 0; n < kLfCols; ++n) dacc[n] = 0.f;
+    const float2* V = a.Vf[m] + static_cast<size_t>(rb0 + rt0) * K3;
+    const double* kh = a.khat[m];
+    const int nchunk = (K3 + kLfChunk - 1) / kLfChunk;
+    for (int c = 0; c < nchunk && ok; ++c, ++gc) {
+      const int st = gc & 1;
+      uint32_t* const Ah = stage0 + st * kStage;
+      uint32_t* const Al = Ah + kLfStageA;
+      uint32_t* const Bh = Ah + 2 * kLfStageA;
+      uint32_t* const Bl = Bh + kLfStageB;
+      if (gc >= 2)  // the stage's previous MMAs (chunk gc - 2) are done
+        ok = __syncthreads_and(mbar_wait(bar + st, ((gc - 2) >> 1) & 1, a.status)) != 0;
+      if (!ok) break;
+      if (c >= 2) {  // chunk c - 2 of this medium is in the stage's accumulator
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        drain(st);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      }
+      const int e0 = c * kLfChunk;
+      // A: 32 RWGs x 16 entries, 4 items per thread (16 consecutive entries of one RWG per 16 threads)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int ep = tid & 15, ri = (tid >> 4) + 8 * i, e = e0 + ep;
+        float2 v = make_float2(0.f, 0.f), w = make_float2(0.f, 0.f);
+        if (ri < nt && e < K3) {
+          const int cc = e / K, k = e - cc * K;
+          const float2* vr = V + static_cast<size_t>(ri) * K3 + k;
+          const float2 v0 = __ldg(vr), v1 = __ldg(vr + K), v2 = __ldg(vr + 2 * K);
+          const float ax = static_cast<float>(-__ldg(kh + k)), ay = static_cast<float>(-__ldg(kh + K + k)),
+                      az = static_cast<float>(-__ldg(kh + 2 * K + k));
+          v = cc == 0 ? v0 : (cc == 1 ? v1 : v2);
+          if (cc == 0)
+            w = make_float2(v2.x * ay - v1.x * az, v2.y * ay - v1.y * az);
+          else if (cc == 1)
+            w = make_float2(v0.x * az - v2.x * ax, v0.y * az - v2.y * ax);
+          else
+            w = make_float2(v1.x * ax - v0.x * ay, v1.y * ax - v0.y * ay);
+        }
+        const float val[4][2] = {{v.x, -v.y}, {v.y, v.x}, {w.x, -w.y}, {w.y, w.x}};
+#pragma unroll
+        for (int tt = 0; tt < 4; ++tt)
+#pragma unroll
+          for (int s2 = 0; s2 < 2; ++s2) {
+            const uint32_t hi = tf32_rna(val[tt][s2]), lo = tf32_rna(val[tt][s2] - __uint_as_float(hi));
+            const uint32_t o = kmajor_offset(4 * ri + tt, 2 * ep + s2, kLfRows) >> 2;
+            Ah[o] = hi;
+            Al[o] = lo;
+          }
+      }
+      // B: 32 columns x 16 entries, 4 per thread
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int ep = tid & 15, col = (tid >> 4) + 8 * i, e = e0 + ep;
+        const int part = col >> 4, j = col & 15;
+        float2 v = make_float2(0.f, 0.f);
+        if (j < R && e < K3) v = __ldg(a.Bm[m][j] + static_cast<size_t>(b) * 2 * K3 + part * K3 + e);
+        const uint32_t hr = tf32_rna(v.x), hi = tf32_rna(v.y);
+        const uint32_t o0 = kmajor_offset(col, 2 * ep, kLfCols) >> 2, o1 = kmajor_offset(col, 2 * ep + 1, kLfCols) >> 2;
+        Bh[o0] = hr;
+        Bl[o0] = tf32_rna(v.x - __uint_as_float(hr));
+        Bh[o1] = hi;
+        Bl[o1] = tf32_rna(v.y - __uint_as_float(hi));
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (tid == 0) {
+#pragma unroll
+        for (int ks = 0; ks < 2 * kLfChunk / 8; ++ks) {
+          const uint64_t ah = smem_desc(smem_addr(Ah) + ks * kLfRows * 32, kLfRows * 16, 128);
+          const uint64_t al = smem_desc(smem_addr(Al) + ks * kLfRows * 32, kLfRows * 16, 128);
+          const uint64_t bh = smem_desc(smem_addr(Bh) + ks * kLfCols * 32, kLfCols * 16, 128);
+          const uint64_t bl = smem_desc(smem_addr(Bl) + ks * kLfCols * 32, kLfCols * 16, 128);
+          const uint32_t acc = tmem + st * kLfCols;
+          mma_tf32(acc, ah, bh, idesc, ks > 0 ? 1u : 0u);
+          mma_tf32(acc, ah, bl, idesc, 1u);
+          mma_tf32(acc, al, bh, idesc, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(bar + st))
+                     : "memory");
+      }
+    }
+    if (!ok) break;
+    // the medium's last (up to) two chunks: their accumulators
+    ok = __syncthreads_and(mbar_wait(bar + ((gc - 1) & 1), ((gc - 1) >> 1) & 1, a.status)) != 0;
+    if (!ok) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (nchunk >= 2) drain((gc - 2) & 1);
+    drain((gc - 1) & 1);
+    const float* d = dacc;
+    float2 LJ[4], KJ[4], LM[4], KM[4];
+    const int g0 = lane & ~3;
+#pragma unroll
+    for (int n = 0; n < kLfCols; ++n) {
+      const float lre = __shfl_sync(0xffffffffu, d[n], g0), lim = __shfl_sync(0xffffffffu, d[n], g0 + 1);
+      const float kre = __shfl_sync(0xffffffffu, d[n], g0 + 2), kim = __shfl_sync(0xffffffffu, d[n], g0 + 3);
+      if ((n & 3) == t) {
+        if (n < 16) {
+          LJ[n >> 2] = make_float2(lre, lim);
+          KJ[n >> 2] = make_float2(kre, kim);
+        } else {
+          LM[(n - 16) >> 2] = make_float2(lre, lim);
+          KM[(n - 16) >> 2] = make_float2(kre, kim);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (m == 0) {
+        wj[q] = cmul(a.c1, csub(LJ[q], KM[q]));
+        wm[q] = cmul(a.c1, cadd(KJ[q], LM[q]));
+      } else {
+        wj[q] = cadd(wj[q], cmul(a.c2, csub(cmul(a.etai, LJ[q]), KM[q])));
+        wm[q] = cadd(wm[q], cmul(a.c2, cadd(KJ[q], cdiv(LM[q], a.etai))));
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // every warp has read TMEM before the next medium's MMAs overwrite it
+  }
+  if (ok) {
+    const int ri = 8 * warp + rr;
+    if (ri < nt) {
+      const int id = a.leaf_rwg[rb0 + rt0 + ri];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = 4 * q + t;
+        if (j < R) {
+          double2* w = a.W + j * a.ldw;
+          w[id] = cadd(w[id], c2(static_cast<double>(wj[q].x), static_cast<double>(wj[q].y)));
+          w[a.N + id] = cadd(w[a.N + id], c2(static_cast<double>(wm[q].x), static_cast<double>(wm[q].y)));
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kLfCols)
+                 : "memory");
+  }
+}
+
 }  // namespace
 
 size_t agg_tc_smem_bytes(int kmax) {
-  return static_cast<size_t>(kTcRows + kTcCols) * kmax * 2 * sizeof(uint32_t) + 2 * sizeof(uint64_t);
+  return static_cast<size_t>(kTcRows + kTcCols) * kmax * 2 * sizeof(uint32_t) + 2 * sizeof(uint64_t) +
+         static_cast<size_t>(kmax) * sizeof(int);
+}
+
+void launch_leaf_tc(const Plan& P, const LeafTcArg& a, cudaStream_t s) {
+  if (a.R < 1 || a.R > 16) throw std::invalid_argument("tensor-core far-field testing: 1 <= R <= 16");
+  const size_t smem = 2 * 2 * (kLfStageA + kLfStageB) * sizeof(uint32_t) + 4 * sizeof(uint64_t);
+  MLFMA_CUDA(
+      cudaFuncSetAttribute(leaf_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  const int tiles = (P.max_leaf_rwgs + 31) / 32;
+  leaf_tc_kernel<<<dim3(P.lv[P.maxL].B, tiles), 128, smem, s>>>(a);
+  MLFMA_CUDA(cudaGetLastError());
 }
 
 bool agg_tc_supported(const Plan& P, int R) {

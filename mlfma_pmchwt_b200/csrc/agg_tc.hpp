@@ -21,8 +21,29 @@ struct AggTcArg {
   int* status;
 };
 
+// Far-field testing of the batched complex64 apply on the tensor cores: per
+// leaf box and tile of 32 RWGs, [Vf; (-khat) x Vf] (rows) times the box's Bm
+// (J and M columns of every slot), contracted over the 3K pattern entries;
+// adds c1 (L1J - K1M) + c2 (etai L2J - K2M) and c1 (K1J + L1M) + c2 (K2J +
+// L2M / etai) into w (Code/MLFMM.cpp:285-351), whose near-field rows are
+// already there.
+struct LeafTcArg {
+  const float2* Vf[2];           // receive patterns, complex64 [N][3K] (leaf order)
+  const float2* Bm[2][kBatchSlots];  // leaf-level Bm of each slot, [B][6][K]
+  const double* khat[2];         // [3][K]
+  int K[2];
+  const int* leaf_ptr;
+  const int* leaf_rwg;
+  double2* W;                    // w_j at W + j * ldw
+  long long ldw;
+  float2 c1, c2, etai;
+  int N, R;
+  int* status;
+};
+
 bool agg_tc_supported(const Plan& P, int R);
 size_t agg_tc_smem_bytes(int kmax);
 void launch_agg_tc(const Plan& P, const AggTcArg& a, cudaStream_t s);
+void launch_leaf_tc(const Plan& P, const LeafTcArg& a, cudaStream_t s);
 
 }  // namespace mlfma

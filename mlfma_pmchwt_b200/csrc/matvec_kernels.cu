@@ -1329,7 +1329,9 @@ struct LeafBatchArg {
 };
 
 // One warp per (RWG, group of RB right-hand sides).
-template <class C, int RB>
+// kFar = false: the near-field rows alone (the far field is added by the
+// tensor-core testing kernel).
+template <class C, int RB, bool kFar = true>
 __global__ void __launch_bounds__(kThreads) leaf_out_batch_kernel(LeafBatchArg<C> a) {
   using Rl = typename Cx<C>::real;
   const int lane = threadIdx.x & 31;
@@ -1340,7 +1342,9 @@ __global__ void __launch_bounds__(kThreads) leaf_out_batch_kernel(LeafBatchArg<C
   const int b = a.rwg_box[id];
   C wj[RB], wm[RB];
 #pragma unroll
-  for (int m = 0; m < 2; ++m) {
+  for (int j = 0; j < RB; ++j) wj[j] = wm[j] = Cx<C>::zero();
+#pragma unroll
+  for (int m = 0; m < (kFar ? 2 : 0); ++m) {
     const int K = a.K[m];
     const C* V = a.Vf[m] + static_cast<size_t>(r) * 3 * K;
     const double* kh = a.khat[m];
@@ -1743,7 +1747,7 @@ void apply_batch_fixed(Plan& P, int R, const double2* X, long long ldx, double2*
     ag.R = rn;
     bool on_tensor_cores = false;
     if constexpr (std::is_same<C, float2>::value) {
-      if (P.tuning.batch_agg == 1 && agg_tc_supported(P, rn)) {
+      if (P.tuning.batch_tc == 1 && agg_tc_supported(P, rn)) {
         AggTcArg t{};
         for (int m = 0; m < 2; ++m) {
           t.Vs[m] = reinterpret_cast<const float*>(ag.Vs[m]);
@@ -1784,9 +1788,35 @@ void apply_batch_fixed(Plan& P, int R, const double2* X, long long ldx, double2*
     lb.ldw = ldw;
     lb.R = rn;
     const int warps = kThreads / 32;
-    leaf_out_batch_kernel<C, kLeafRB>
-        <<<dim3((P.N + warps - 1) / warps, (rn + kLeafRB - 1) / kLeafRB), kThreads, 0, s>>>(lb);
-    MLFMA_CUDA(cudaGetLastError());
+    const dim3 grid((P.N + warps - 1) / warps, (rn + kLeafRB - 1) / kLeafRB);
+    if (on_tensor_cores) {
+      // near-field rows first (writing w), then the far field on the tensor cores (adding)
+      leaf_out_batch_kernel<C, kLeafRB, false><<<grid, kThreads, 0, s>>>(lb);
+      MLFMA_CUDA(cudaGetLastError());
+      if constexpr (std::is_same<C, float2>::value) {
+        LeafTcArg t{};
+        for (int m = 0; m < 2; ++m) {
+          t.Vf[m] = lb.Vf[m];
+          t.khat[m] = lb.khat[m];
+          t.K[m] = lb.K[m];
+          for (int j = 0; j < rn; ++j) t.Bm[m][j] = lb.Bm[m][j];
+        }
+        t.leaf_ptr = P.d_leaf_ptr;
+        t.leaf_rwg = P.d_leaf_rwg;
+        t.W = lb.W;
+        t.ldw = ldw;
+        t.c1 = lb.c1;
+        t.c2 = lb.c2;
+        t.etai = lb.etai;
+        t.N = P.N;
+        t.R = rn;
+        t.status = P.d_status;
+        launch_leaf_tc(P, t, s);
+      }
+    } else {
+      leaf_out_batch_kernel<C, kLeafRB><<<grid, kThreads, 0, s>>>(lb);
+      MLFMA_CUDA(cudaGetLastError());
+    }
   }
 }
 

@@ -128,7 +128,7 @@ struct Tuning {
                                // 3: separable in registers, 4-row bands per thread
   int agg_variant = 0;         // 0: thread per (box, direction); 1: CTA per (box, medium) streaming
                                //    the box's contiguous pattern block
-  int batch_agg = 1;           // batched complex64 aggregation: 0 CUDA cores; 1 tcgen05 tensor cores
+  int batch_tc = 1;            // batched complex64 leaf aggregation and far-field testing: 0 CUDA cores; 1 tcgen05
                                //    (3xTF32 split, TMEM accumulators)
   int leaf_variant = 0;        // 0: near field inside the leaf kernel; 1: near field on its own
                                //    stream from the start of the apply, the leaf kernel adds the far field

@@ -72,10 +72,10 @@ def test_fp64_plan_rejects_mixed_calls(case_files):
 
 @pytest.mark.parametrize("R", [1, 5, 16])
 def test_tensor_core_batched_aggregation(case_files, R):
-    """The batched complex64 apply with the leaf aggregation on the tensor
-    cores (tcgen05, TF32 high/low split) against the same apply with the
-    CUDA-core aggregation (agreement at complex64 rounding) and against the
-    FP64 operator (the complex64 operator's own error)."""
+    """The batched complex64 apply with the leaf aggregation and far-field
+    testing on the tensor cores (tcgen05, TF32 high/low split) against the
+    same apply on the CUDA cores (agreement at complex64 rounding) and
+    against the FP64 operator (the complex64 operator's own error)."""
     import torch
     from mlfma_pmchwt_b200 import mesh as M
     op = mixed_op(case_files, "sphere_s3_lossy")
@@ -84,13 +84,13 @@ def test_tensor_core_batched_aggregation(case_files, R):
     X = torch.from_numpy(np.stack([M.unit_disk_vector(op.n, 60 + j) for j in range(R)])).cuda()
     outs = {}
     for v in (0, 1):
-        op.set_tuning("batch_agg.variant", v)
+        op.set_tuning("batch_tc.variant", v)
         W = torch.full_like(X, float("nan"))
         torch.cuda.synchronize()
         op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr())
         torch.cuda.synchronize()
         outs[v] = W.cpu().numpy()
-    op.set_tuning("batch_agg.variant", 0)
+    op.set_tuning("batch_tc.variant", 0)
     assert op.device_status() == 0
     ref = op.apply_batch(X.cpu().numpy())
     for j in range(R):
