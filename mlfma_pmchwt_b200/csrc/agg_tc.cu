@@ -230,12 +230,15 @@ __global__ void __launch_bounds__(128, 1) agg_tc_kernel(const __grid_constant__ 
 // imaginary row (a_im, a_re), so that D[real row] and D[imaginary row] are
 // the real and imaginary parts of sum_e a_e b_e. B: column part * 16 + j is
 // Bm_j of the box (part 0 the J half, 1 the M half), whose interleaved
-// complex layout already is the real K order. The K extent streams through
-// two shared-memory stages of 16 entries (32 real) each: the MMAs of one
-// stage run while the threads fill the other.
+// complex layout already is the real K order. The contraction runs over
+// chunks of 4 directions (their 3 x 4 entries, 24 real K; a thread builds one
+// RWG's Vf and W at one direction from one set of loads) through two
+// shared-memory stages: the MMAs of one stage run while the threads fill the
+// other.
 constexpr int kLfRows = 128;      // 32 RWGs x 4 rows
 constexpr int kLfCols = 32;       // 2 parts x 16 slots
-constexpr int kLfChunk = 16;      // complex entries per stage (32 real K)
+constexpr int kLfDirs = 4;        // directions per stage: 3 x 4 complex entries (24 real K)
+constexpr int kLfChunk = 3 * kLfDirs;
 constexpr int kLfStageA = kLfRows * 2 * kLfChunk;  // tf32 values per A operand stage
 constexpr int kLfStageB = kLfCols * 2 * kLfChunk;
 
@@ -295,7 +298,7 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
     for (int n = 0; n < kLfCols; ++n) dacc[n] = 0.f;
     const float2* V = a.Vf[m] + static_cast<size_t>(rb0 + rt0) * K3;
     const double* kh = a.khat[m];
-    const int nchunk = (K3 + kLfChunk - 1) / kLfChunk;
+    const int nchunk = (K + kLfDirs - 1) / kLfDirs;
     for (int c = 0; c < nchunk && ok; ++c, ++gc) {
       const int st = gc & 1;
       uint32_t* const Ah = stage0 + st * kStage;
@@ -310,44 +313,47 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
         drain(st);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       }
-      const int e0 = c * kLfChunk;
-      // A: 32 RWGs x 16 entries, 4 items per thread (16 consecutive entries of one RWG per 16 threads)
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int ep = tid & 15, ri = (tid >> 4) + 8 * i, e = e0 + ep;
-        float2 v = make_float2(0.f, 0.f), w = make_float2(0.f, 0.f);
-        if (ri < nt && e < K3) {
-          const int cc = e / K, k = e - cc * K;
+      // stage entries: (component cc, direction k0 + kk) at complex index cc * kLfDirs + kk
+      const int k0 = c * kLfDirs;
+      {  // A: one (RWG, direction) per thread: the 3 components of Vf and of W = (-khat) x Vf
+        const int kk = tid & (kLfDirs - 1), ri = tid / kLfDirs, k = k0 + kk;
+        float2 v[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        float2 w[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        if (ri < nt && k < K) {
           const float2* vr = V + static_cast<size_t>(ri) * K3 + k;
-          const float2 v0 = __ldg(vr), v1 = __ldg(vr + K), v2 = __ldg(vr + 2 * K);
+          v[0] = __ldg(vr);
+          v[1] = __ldg(vr + K);
+          v[2] = __ldg(vr + 2 * K);
           const float ax = static_cast<float>(-__ldg(kh + k)), ay = static_cast<float>(-__ldg(kh + K + k)),
                       az = static_cast<float>(-__ldg(kh + 2 * K + k));
-          v = cc == 0 ? v0 : (cc == 1 ? v1 : v2);
-          if (cc == 0)
-            w = make_float2(v2.x * ay - v1.x * az, v2.y * ay - v1.y * az);
-          else if (cc == 1)
-            w = make_float2(v0.x * az - v2.x * ax, v0.y * az - v2.y * ax);
-          else
-            w = make_float2(v1.x * ax - v0.x * ay, v1.y * ax - v0.y * ay);
+          w[0] = make_float2(v[2].x * ay - v[1].x * az, v[2].y * ay - v[1].y * az);
+          w[1] = make_float2(v[0].x * az - v[2].x * ax, v[0].y * az - v[2].y * ax);
+          w[2] = make_float2(v[1].x * ax - v[0].x * ay, v[1].y * ax - v[0].y * ay);
         }
-        const float val[4][2] = {{v.x, -v.y}, {v.y, v.x}, {w.x, -w.y}, {w.y, w.x}};
 #pragma unroll
-        for (int tt = 0; tt < 4; ++tt)
+        for (int cc = 0; cc < 3; ++cc) {
+          const int ep = cc * kLfDirs + kk;
+          const float val[4][2] = {{v[cc].x, -v[cc].y}, {v[cc].y, v[cc].x}, {w[cc].x, -w[cc].y}, {w[cc].y, w[cc].x}};
 #pragma unroll
-          for (int s2 = 0; s2 < 2; ++s2) {
-            const uint32_t hi = tf32_rna(val[tt][s2]), lo = tf32_rna(val[tt][s2] - __uint_as_float(hi));
-            const uint32_t o = kmajor_offset(4 * ri + tt, 2 * ep + s2, kLfRows) >> 2;
-            Ah[o] = hi;
-            Al[o] = lo;
-          }
+          for (int tt = 0; tt < 4; ++tt)
+#pragma unroll
+            for (int s2 = 0; s2 < 2; ++s2) {
+              const uint32_t hi = tf32_rna(val[tt][s2]), lo = tf32_rna(val[tt][s2] - __uint_as_float(hi));
+              const uint32_t o = kmajor_offset(4 * ri + tt, 2 * ep + s2, kLfRows) >> 2;
+              Ah[o] = hi;
+              Al[o] = lo;
+            }
+        }
       }
-      // B: 32 columns x 16 entries, 4 per thread
+      // B: 32 columns x 12 entries, 3 per thread
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int ep = tid & 15, col = (tid >> 4) + 8 * i, e = e0 + ep;
+      for (int i = 0; i < 3; ++i) {
+        const int q = tid + 128 * i;  // < 384
+        const int ep = q % kLfChunk, col = q / kLfChunk;
+        const int cc = ep / kLfDirs, k = k0 + (ep - cc * kLfDirs);
         const int part = col >> 4, j = col & 15;
         float2 v = make_float2(0.f, 0.f);
-        if (j < R && e < K3) v = __ldg(a.Bm[m][j] + static_cast<size_t>(b) * 2 * K3 + part * K3 + e);
+        if (j < R && k < K) v = __ldg(a.Bm[m][j] + static_cast<size_t>(b) * 2 * K3 + part * K3 + cc * K + k);
         const uint32_t hr = tf32_rna(v.x), hi = tf32_rna(v.y);
         const uint32_t o0 = kmajor_offset(col, 2 * ep, kLfCols) >> 2, o1 = kmajor_offset(col, 2 * ep + 1, kLfCols) >> 2;
         Bh[o0] = hr;
