@@ -45,10 +45,7 @@ std::vector<double> fp64_residuals(Plan& P, const std::vector<int>& list, const 
     for (int j = 0; j < rn; ++j)
       MLFMA_CUDA(cudaMemcpyAsync(Xd + j * n, X + list[g0 + j] * n, n * sizeof(double2), cudaMemcpyHostToDevice,
                                  P.stream));
-    if (rn == 1)
-      apply_device(P, Xd, Wd, P.stream);
-    else
-      apply_batch_device(P, rn, Xd, n, Wd, n, P.stream);
+    for (int j = 0; j < rn; ++j) apply_device(P, Xd + j * n, Wd + j * n, P.stream);
     std::vector<C> w(static_cast<size_t>(rn) * n);
     MLFMA_CUDA(cudaMemcpyAsync(w.data(), Wd, w.size() * sizeof(double2), cudaMemcpyDeviceToHost, P.stream));
     MLFMA_CUDA(cudaStreamSynchronize(P.stream));
