@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(128, 1) agg_tc_kernel(const __grid_constant__ 
 }
 
 // Far-field testing (see LeafTcArg). One real GEMM per (box, 32-RWG tile,
-// medium): A rows 4 rr + t for RWG rr, t = 0 / 1 the real / imaginary row of
+// medium): A rows 32 t + rr for RWG rr, t = 0 / 1 the real / imaginary row of
 // Vf and t = 2 / 3 those of W = (-khat) x Vf, over real K = 2 x 3K (entry e
 // gives columns 2e (re) and 2e + 1 (im)): a real row holds (a_re, -a_im), an
 // imaginary row (a_im, a_re), so that D[real row] and D[imaginary row] are
@@ -245,7 +245,7 @@ constexpr int kLfStageB = kLfCols * 2 * kLfChunk;
 __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__ LeafTcArg a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int b = blockIdx.x, tile = blockIdx.y;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int rb0 = a.leaf_ptr[b], nb = a.leaf_ptr[b + 1] - rb0;
   const int rt0 = tile * 32;
   if (rt0 >= nb) return;
@@ -272,8 +272,8 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
   const uint32_t tmem = *tslot;
   constexpr uint32_t idesc = idesc_tf32(kLfRows, kLfCols);
   const int R = a.R;
-  const int rr = lane >> 2, t = lane & 3;  // epilogue: RWG (of this warp's 8) and row kind of this lane
-  float2 wj[4], wm[4];                     // slots j = 4 jj + t of RWG 8 warp + rr
+  const int t = tid & 3;  // epilogue: slots j = 4 q + t of RWG tid / 4
+  float2 wj[4], wm[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) wj[q] = wm[q] = make_float2(0.f, 0.f);
   // Each chunk's MMAs start a fresh accumulator (TMEM columns 32 x stage);
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
       // stage entries: (component cc, direction k0 + kk) at complex index cc * kLfDirs + kk
       const int k0 = c * kLfDirs;
       {  // A: one (RWG, direction) per thread: the 3 components of Vf and of W = (-khat) x Vf
-        const int kk = tid & (kLfDirs - 1), ri = tid / kLfDirs, k = k0 + kk;
+        const int ri = tid & 31, kk = tid >> 5, k = k0 + kk;
         float2 v[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         float2 w[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         if (ri < nt && k < K) {
@@ -335,14 +335,14 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
           const int ep = cc * kLfDirs + kk;
           const float val[4][2] = {{v[cc].x, -v[cc].y}, {v[cc].y, v[cc].x}, {w[cc].x, -w[cc].y}, {w[cc].y, w[cc].x}};
 #pragma unroll
-          for (int tt = 0; tt < 4; ++tt)
-#pragma unroll
-            for (int s2 = 0; s2 < 2; ++s2) {
-              const uint32_t hi = tf32_rna(val[tt][s2]), lo = tf32_rna(val[tt][s2] - __uint_as_float(hi));
-              const uint32_t o = kmajor_offset(4 * ri + tt, 2 * ep + s2, kLfRows) >> 2;
-              Ah[o] = hi;
-              Al[o] = lo;
-            }
+          for (int tt = 0; tt < 4; ++tt) {
+            // row tt * 32 + ri: the 8 rows of a core matrix come from 8 neighbouring lanes
+            const uint32_t h0 = tf32_rna(val[tt][0]), h1 = tf32_rna(val[tt][1]);
+            const uint32_t l0 = tf32_rna(val[tt][0] - __uint_as_float(h0)), l1 = tf32_rna(val[tt][1] - __uint_as_float(h1));
+            const uint32_t o = kmajor_offset(tt * 32 + ri, 2 * ep, kLfRows) >> 2;  // 8-byte aligned pair
+            *reinterpret_cast<uint2*>(Ah + o) = make_uint2(h0, h1);
+            *reinterpret_cast<uint2*>(Al + o) = make_uint2(l0, l1);
+          }
         }
       }
       // B: 32 columns x 12 entries, 3 per thread
@@ -355,11 +355,10 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
         float2 v = make_float2(0.f, 0.f);
         if (j < R && k < K) v = __ldg(a.Bm[m][j] + static_cast<size_t>(b) * 2 * K3 + part * K3 + cc * K + k);
         const uint32_t hr = tf32_rna(v.x), hi = tf32_rna(v.y);
-        const uint32_t o0 = kmajor_offset(col, 2 * ep, kLfCols) >> 2, o1 = kmajor_offset(col, 2 * ep + 1, kLfCols) >> 2;
-        Bh[o0] = hr;
-        Bl[o0] = tf32_rna(v.x - __uint_as_float(hr));
-        Bh[o1] = hi;
-        Bl[o1] = tf32_rna(v.y - __uint_as_float(hi));
+        const uint32_t o = kmajor_offset(col, 2 * ep, kLfCols) >> 2;  // 8-byte aligned pair
+        *reinterpret_cast<uint2*>(Bh + o) = make_uint2(hr, hi);
+        *reinterpret_cast<uint2*>(Bl + o) =
+            make_uint2(tf32_rna(v.x - __uint_as_float(hr)), tf32_rna(v.y - __uint_as_float(hi)));
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
@@ -388,22 +387,21 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (nchunk >= 2) drain((gc - 2) & 1);
     drain((gc - 1) & 1);
-    const float* d = dacc;
-    float2 LJ[4], KJ[4], LM[4], KM[4];
-    const int g0 = lane & ~3;
+    // warp tt holds row kind tt of all 32 RWGs (lane = RWG): regroup per RWG
+    // through shared memory (the stages are idle), E[column][row]
+    float* E = reinterpret_cast<float*>(stage0);
 #pragma unroll
-    for (int n = 0; n < kLfCols; ++n) {
-      const float lre = __shfl_sync(0xffffffffu, d[n], g0), lim = __shfl_sync(0xffffffffu, d[n], g0 + 1);
-      const float kre = __shfl_sync(0xffffffffu, d[n], g0 + 2), kim = __shfl_sync(0xffffffffu, d[n], g0 + 3);
-      if ((n & 3) == t) {
-        if (n < 16) {
-          LJ[n >> 2] = make_float2(lre, lim);
-          KJ[n >> 2] = make_float2(kre, kim);
-        } else {
-          LM[(n - 16) >> 2] = make_float2(lre, lim);
-          KM[(n - 16) >> 2] = make_float2(kre, kim);
-        }
-      }
+    for (int n = 0; n < kLfCols; ++n) E[n * kLfRows + tid] = dacc[n];
+    __syncthreads();
+    const int er = tid >> 2;  // RWG of this thread's outputs
+    float2 LJ[4], KJ[4], LM[4], KM[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = 4 * q + t;
+      LJ[q] = make_float2(E[j * kLfRows + er], E[j * kLfRows + 32 + er]);
+      KJ[q] = make_float2(E[j * kLfRows + 64 + er], E[j * kLfRows + 96 + er]);
+      LM[q] = make_float2(E[(16 + j) * kLfRows + er], E[(16 + j) * kLfRows + 32 + er]);
+      KM[q] = make_float2(E[(16 + j) * kLfRows + 64 + er], E[(16 + j) * kLfRows + 96 + er]);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -419,7 +417,7 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
     __syncthreads();  // every warp has read TMEM before the next medium's MMAs overwrite it
   }
   if (ok) {
-    const int ri = 8 * warp + rr;
+    const int ri = tid >> 2;
     if (ri < nt) {
       const int id = a.leaf_rwg[rb0 + rt0 + ri];
 #pragma unroll
