@@ -379,6 +379,53 @@ def bodies_study(args, local: int) -> dict:
             "converged": sum(r["converged"] for r in rows), "per_body": rows}
 
 
+def batched_apply_study(args, local: int, wl: dict) -> dict:
+    """The batched complex64 apply of 16 right-hand sides on the workload's
+    sphere (mixed-precision plan): per-batch CUDA-event time with the leaf
+    aggregation and far-field testing on the tensor cores (batch_tc.variant
+    1) and on the CUDA cores (0), against 16 single complex64 applies, and
+    the tensor-core rows' relative difference from the FP64 operator."""
+    import torch
+    from mlfma_pmchwt_b200 import MLFMM
+    from mlfma_pmchwt_b200 import mesh as M
+    op = MLFMM(M.icosphere(wl["sub"], wl["radius"]), freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"],
+               device=local, precision="mixed")
+    R = 16
+    X = torch.from_numpy(np.stack([M.unit_disk_vector(op.n, 60 + j) for j in range(R)])).cuda(local)
+    W = torch.empty_like(X)
+    stream = torch.cuda.Stream(local)
+    sp = stream.cuda_stream
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(local)
+        return e0.elapsed_time(e1) / reps
+
+    out = {"workload": wl["name"], "rhs": R, "ms_per_batch": {}}
+    for v in (1, 0):
+        op.set_tuning("batch_tc.variant", v)
+        out["ms_per_batch"]["tensor_cores" if v else "cuda_cores"] = round(
+            timed(lambda: op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp), 3), 3)
+    op.set_tuning("batch_tc.variant", 1)
+    out["ms_per_batch"]["16_single_applies"] = round(16 * timed(
+        lambda: op.apply_mixed_device(X[0].data_ptr(), W[0].data_ptr(), sp), 10), 3)
+    op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp)
+    torch.cuda.synchronize(local)
+    Wt = W.cpu().numpy()
+    ref = op.apply_batch(X.cpu().numpy())
+    out["rel_diff_vs_fp64_max"] = float(max(np.linalg.norm(Wt[j] - ref[j]) / np.linalg.norm(ref[j]) for j in range(R)))
+    out["device_status"] = op.device_status()
+    op.close()
+    return out
+
+
 def run_product(args):
     import torch
     from mlfma_pmchwt_b200 import MLFMM
@@ -388,6 +435,10 @@ def run_product(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     wl = workload(args)
+    if args.batched_only:  # the batched-apply study alone (small enough for profiler captures)
+        if rank == 0:
+            print(json.dumps({"batched_apply": batched_apply_study(args, local, wl)}))
+        return 0
     m = M.icosphere(wl["sub"], wl["radius"])
     t0 = time.perf_counter()
     op = MLFMM(m, freq=FREQ, eps_r=wl["eps"], leaf_coeff=wl["leaf"], device=local,
@@ -562,6 +613,8 @@ def run_product(args):
             "roofline": roofline, "clocks": clk}
     if mixed:
         line["mixed_precision"] = mixed
+    if args.mixed and world == 1:
+        line["batched_apply"] = batched_apply_study(args, local, wl)
     if args.rhs > 0 and world == 1:
         line["multi_rhs"] = multi_rhs_study(args, local)
     if args.bodies and world == 1:
@@ -604,6 +657,8 @@ def main(argv=None):
     ap.add_argument("--bodies", action="store_true", help="also run the 24-body uneven batch study")
     ap.add_argument("--no-mixed", dest="mixed", action="store_false",
                     help="skip the complex64 (mixed-precision) operator and solve")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the 16-right-hand-side batched complex64 apply study and print its record")
     ap.add_argument("--bodies-workers", type=int, default=4,
                     help="bodies solved at once by the --bodies study (host threads, one plan each)")
     ap.add_argument("--tuning", default="auto",
