@@ -69,6 +69,105 @@ __global__ void __launch_bounds__(128) near_apply_kernel(NearArg<Z> a) {
   }
 }
 
+// Device state of the preconditioner's inner GMRES: its Hessenberg matrix,
+// rotations and right-hand side live on the GPU, so that the inner steps run
+// without a host round trip.
+struct InnerDev {
+  double2* H;   // [(inner + 1) x inner], column-major, ld = inner + 1
+  double2* cs;  // [inner] rotations
+  double2* sn;
+  double2* g;   // [inner + 1] rotated right-hand side
+  double2* y;   // [inner] solution of the triangular system
+  double2* h1;  // [inner + 1] coefficients of the two Gram-Schmidt passes
+  double2* h2;
+  double2* hn2; // [1] ||u||^2 after the projections (real part)
+  double* sc;   // [0] beta, [1] scale of the next basis vector, [2] 1 / beta
+  int* flags;   // [0] breakdown, [1] columns in use
+};
+
+__device__ __forceinline__ double2 dconj(double2 a) { return c2(a.x, -a.y); }
+
+// The rotations of Code/GMRES.h:22-48 (as blas1::givens_make / givens_apply).
+__device__ void dgivens_make(double2 a, double2 b, double2& c, double2& s) {
+  const double eps = 1e-16;
+  if (sqrt(b.x * b.x + b.y * b.y) < eps) {
+    c = c2(1.0, 0.0);
+    s = c2(0.0, 0.0);
+  } else if (sqrt(a.x * a.x + a.y * a.y) < eps) {
+    c = c2(0.0, 0.0);
+    s = c2(1.0, 0.0);
+  } else {
+    const double r = sqrt(a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y);
+    c = c2(a.x / r, a.y / r);
+    s = c2(b.x / r, b.y / r);
+  }
+}
+__device__ void dgivens_apply(double2& x, double2& y, double2 c, double2 s) {
+  const double2 t = cadd(cmul(dconj(c), x), cmul(dconj(s), y));
+  y = cadd(cmul(c2(-s.x, -s.y), x), cmul(c, y));
+  x = t;
+}
+
+// beta = ||v|| from the norm partials; g = (beta, 0, ...); flags cleared
+__global__ void inner_begin(const double2* partial, int nblk, InnerDev d, int inner) {
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += partial[b].x;
+  const double beta = sqrt(s);
+  d.sc[0] = beta;
+  d.sc[2] = beta > 0.0 ? 1.0 / beta : 0.0;
+  for (int i = 0; i <= inner; ++i) d.g[i] = c2(i == 0 ? beta : 0.0, 0.0);
+  d.flags[0] = 0;
+  d.flags[1] = 0;
+}
+
+// column j of H from the Gram-Schmidt coefficients, its rotations, and the
+// scale of the next basis vector (0 after a breakdown)
+__global__ void inner_step(InnerDev d, int j, int ld) {
+  if (d.flags[0]) {
+    d.sc[1] = 0.0;
+    return;
+  }
+  double2* Hj = d.H + static_cast<long long>(j) * ld;
+  for (int i = 0; i <= j; ++i) Hj[i] = cadd(d.h1[i], d.h2[i]);
+  const double hn = sqrt(d.hn2[0].x);
+  Hj[j + 1] = c2(hn, 0.0);
+  for (int i = 0; i < j; ++i) dgivens_apply(Hj[i], Hj[i + 1], d.cs[i], d.sn[i]);
+  d.flags[1] = j + 1;
+  if (hn < 1e-14 * d.sc[0]) {
+    d.flags[0] = 1;
+    d.sc[1] = 0.0;
+    return;
+  }
+  d.sc[1] = 1.0 / hn;
+  dgivens_make(Hj[j], Hj[j + 1], d.cs[j], d.sn[j]);
+  dgivens_apply(Hj[j], Hj[j + 1], d.cs[j], d.sn[j]);
+  Hj[j + 1] = c2(0.0, 0.0);
+  dgivens_apply(d.g[j], d.g[j + 1], d.cs[j], d.sn[j]);
+}
+
+// y = R^{-1} g over the columns in use (Code/GMRES.h:165-182); zero beyond
+__global__ void inner_end(InnerDev d, int ld, int inner) {
+  const int m = d.flags[1];
+  const double eps = 1e-16;
+  for (int i = inner - 1; i >= 0; --i) {
+    if (i >= m) {
+      d.y[i] = c2(0.0, 0.0);
+      continue;
+    }
+    double2 yi = d.g[i];
+    for (int j = i + 1; j < m; ++j) yi = csub(yi, cmul(d.H[i + static_cast<long long>(j) * ld], d.y[j]));
+    const double2 hii = d.H[i + static_cast<long long>(i) * ld];
+    d.y[i] = sqrt(hii.x * hii.x + hii.y * hii.y) > eps ? cdiv(yi, hii) : c2(0.0, 0.0);
+  }
+}
+
+// dst = src * s[0]
+__global__ void scale_by(const double2* __restrict__ src, const double* s, double2* __restrict__ dst, long long n) {
+  const double a = *s;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = cscale(src[i], a);
+}
+
 // Upper-triangular solve of the rotated least-squares system (Code/GMRES.h:165-182).
 void back_substitute(const std::vector<C>& H, int ld, const std::vector<C>& s, int m, std::vector<C>& y) {
   const double eps = 1e-16;
@@ -146,36 +245,79 @@ bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, d
   // z = approximate solution of Z_near z = v by inner_its GMRES steps from
   // zero, with the complex64 copy of Z_near (the outer flexible GMRES admits
   // any preconditioner; its operator and residuals stay at the solve's
-  // precision)
-  std::vector<C> Hi(static_cast<size_t>(inner_its + 1) * std::max(inner_its, 1)), ci(inner_its + 1),
-      si(inner_its + 1), gi(inner_its + 1), yi;
-  auto precondition = [&](const double2* v, double2* z) {
-    const double beta = ops.norm(v);
-    blas1::scale<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(v, 1.0 / beta, Q, n);
-    const int ld = inner_its + 1;
-    std::fill(Hi.begin(), Hi.end(), C(0.0));
-    std::fill(gi.begin(), gi.end(), C(0.0));
-    gi[0] = beta;
-    int used = 0;
+  // precision). The inner Hessenberg matrix, rotations and triangular solve
+  // stay on the GPU: the inner steps run without a host round trip.
+  const int ldi = inner_its + 1;
+  InnerDev idv{};
+  if (inner_its > 0) {
+    idv.H = g.get(static_cast<size_t>(ldi) * inner_its);
+    idv.cs = g.get(inner_its);
+    idv.sn = g.get(inner_its);
+    idv.g = g.get(ldi);
+    idv.y = g.get(inner_its);
+    idv.h1 = g.get(ldi);
+    idv.h2 = g.get(ldi);
+    idv.hn2 = g.get(1);
+    idv.sc = reinterpret_cast<double*>(g.get(2));
+    idv.flags = reinterpret_cast<int*>(g.get(1));
+  }
+  auto precondition_launch = [&](const double2* v, double2* z) {
+    blas1::norm2<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(nullptr, v, nullptr, n, ops.part);
+    inner_begin<<<1, 1, 0, s>>>(ops.part, blas1::kBlocks, idv, inner_its);
+    scale_by<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(v, idv.sc + 2, Q, n);
     for (int j = 0; j < inner_its; ++j) {
+      const double2* q = Q + static_cast<long long>(j) * n;
       double2* u = Q + static_cast<long long>(j + 1) * n;
-      near_apply(P, Q + static_cast<long long>(j) * n, u, s, 1);
-      st.near_products++;
-      const double hn = ops.orthogonalise(Q, j + 1, u, hcol);
-      for (int i = 0; i <= j; ++i) Hi[i + j * ld] = hcol[i];
-      Hi[j + 1 + j * ld] = hn;
-      used = j + 1;
-      if (hn < 1e-14 * beta) break;
-      blas1::scale<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(u, 1.0 / hn, u, n);
-      for (int i = 0; i < j; ++i) blas1::givens_apply(Hi[i + j * ld], Hi[i + 1 + j * ld], ci[i], si[i]);
-      blas1::givens_make(Hi[j + j * ld], Hi[j + 1 + j * ld], ci[j], si[j]);
-      blas1::givens_apply(Hi[j + j * ld], Hi[j + 1 + j * ld], ci[j], si[j]);
-      Hi[j + 1 + j * ld] = C(0.0);
-      blas1::givens_apply(gi[j], gi[j + 1], ci[j], si[j]);
+      near_apply(P, q, u, s, 1);
+      const int nv = j + 1;
+      blas1::dots<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, u, ops.part, ops.ldp);
+      blas1::reduce<<<(nv + 63) / 64, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, nv, idv.h1);
+      blas1::project_out<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, idv.h1, u, 0, ops.part, ops.ldp);
+      blas1::dots<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, u, ops.part, ops.ldp);
+      blas1::reduce<<<(nv + 63) / 64, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, nv, idv.h2);
+      blas1::project_out<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, idv.h2, u, 1, ops.part, ops.ldp);
+      blas1::reduce<<<1, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, 1, idv.hn2);
+      inner_step<<<1, 1, 0, s>>>(idv, j, ldi);
+      scale_by<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(u, idv.sc + 1, u, n);
     }
-    back_substitute(Hi, ld, gi, used, yi);
-    MLFMA_CUDA(cudaMemcpyAsync(y, yi.data(), used * sizeof(double2), cudaMemcpyHostToDevice, s));
-    blas1::combine<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, used, y, z, 0);
+    inner_end<<<1, 1, 0, s>>>(idv, ldi, inner_its);
+    blas1::combine<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, inner_its, idv.y, z, 0);
+    MLFMA_CUDA(cudaGetLastError());
+  };
+  // The preconditioner's ~10 launches per inner step are captured once per
+  // solve as a CUDA graph on solve-owned input / output vectors (v copied in,
+  // z out): the same graph serves every basis vector.
+  double2* pv = inner_its > 0 ? g.get(n) : nullptr;
+  double2* pz = inner_its > 0 ? g.get(n) : nullptr;
+  cudaGraphExec_t pgraph = nullptr;
+  struct GraphGuard {
+    cudaGraphExec_t& e;
+    ~GraphGuard() {
+      if (e) cudaGraphExecDestroy(e);
+    }
+  } pguard{pgraph};
+  auto precondition = [&](const double2* v, double2* z) {
+    st.near_products += inner_its;
+    if (!P.tuning.graph) return precondition_launch(v, z);
+    MLFMA_CUDA(cudaMemcpyAsync(pv, v, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    if (pgraph == nullptr) {
+      MLFMA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      try {
+        precondition_launch(pv, pz);
+      } catch (...) {
+        cudaGraph_t gr = nullptr;
+        cudaStreamEndCapture(s, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        throw;
+      }
+      cudaGraph_t gr = nullptr;
+      MLFMA_CUDA(cudaStreamEndCapture(s, &gr));
+      const cudaError_t e = cudaGraphInstantiate(&pgraph, gr, 0);
+      cudaGraphDestroy(gr);
+      MLFMA_CUDA(e);
+    }
+    MLFMA_CUDA(cudaGraphLaunch(pgraph, s));
+    MLFMA_CUDA(cudaMemcpyAsync(z, pz, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
   };
 
   const double eps = 1e-16;
