@@ -118,16 +118,24 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend: str = "nccl"):
+    """One process per GPU (torchrun environment); replicas only: the
+    process group carries the timing barrier and the max over ranks."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
         import torch.distributed as dist
-        backend = "nccl"
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
+
+
+def replica_rate(ms_local: float, steps: int, world: int, device) -> tuple[float, float]:
+    """Whole-job applies per second of N replicas: every rank applies `steps`
+    times; the job's time is the slowest rank's (max over ranks)."""
+    ms_total = allreduce_max(ms_local, world, device)
+    return world * steps / (ms_total / 1000.0), ms_total
 
 
 def allreduce_max(v: float, world: int, device) -> float:
@@ -491,9 +499,8 @@ def run_product(args):
     torch.cuda.synchronize(dev)
     stage_ms, napp = op.stage_times()
     op.profile(False)
-    ms_total = allreduce_max(ms_local, world, dev)
+    value, ms_total = replica_rate(ms_local, args.steps, world, dev)
     ms_per_step = ms_total / args.steps
-    value = world * args.steps / (ms_total / 1000.0)
 
     # end to end through the C ABI with pinned host buffers
     xh = torch.from_numpy(x_host).pin_memory()
