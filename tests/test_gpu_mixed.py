@@ -96,3 +96,34 @@ def test_tensor_core_batched_aggregation(case_files, R):
     for j in range(R):
         assert rel(outs[1][j], outs[0][j]) < 1e-6, j
         assert rel(outs[1][j], ref[j]) < 1e-5, j
+
+
+@pytest.mark.parametrize("leaf,tc_path", [(0.45, True), (0.6, False)])
+def test_tensor_core_batched_apply_large_leaf_boxes(leaf, tc_path):
+    """Leaf boxes of up to 44 RWGs (two 32-RWG tiles in the far-field
+    testing, 48-wide contractions in the aggregation) on the tensor cores;
+    boxes of more than 64 RWGs take the CUDA-core kernels instead."""
+    import torch
+    from mlfma_pmchwt_b200 import MLFMM
+    from mlfma_pmchwt_b200 import mesh as M
+    op = MLFMM(M.icosphere(3, 1.0), freq=FREQ, eps_r=complex(3.0, -0.05), leaf_coeff=leaf, device=0,
+               precision="mixed")
+    ptr, _ = op.leaf_rwgs()
+    assert (np.diff(ptr).max() <= 64) == tc_path and np.diff(ptr).max() > 32
+    R = 5
+    X = torch.from_numpy(np.stack([M.unit_disk_vector(op.n, 80 + j) for j in range(R)])).cuda()
+    outs = {}
+    for v in (0, 1):
+        op.set_tuning("batch_tc.variant", v)
+        W = torch.full_like(X, float("nan"))
+        torch.cuda.synchronize()
+        op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr())
+        torch.cuda.synchronize()
+        outs[v] = W.cpu().numpy()
+    ref = op.apply_batch(X.cpu().numpy())
+    for j in range(R):
+        # same kernels when the tensor-core path is not taken
+        assert rel(outs[1][j], outs[0][j]) < (1e-6 if tc_path else 1e-12), j
+        assert rel(outs[1][j], ref[j]) < 1e-5, j
+    assert op.device_status() == 0
+    op.close()
