@@ -387,6 +387,70 @@ def bodies_study(args, local: int) -> dict:
             "converged": sum(r["converged"] for r in rows), "per_body": rows}
 
 
+def learned_study(args, local: int) -> dict:
+    """Learned preconditioner. Training: (v, P_near v) pairs with white-noise
+    v on --learned-bodies seeded triaxial ellipsoids (mesh.training_ellipsoids:
+    semi-axes 0.5-2 lambda, eps_r 2-6, 15,360 unknowns each), objective
+    |A M v - v|^2 / |v|^2, Adam, all in the library's kernels. Evaluation: the
+    held-out 6 x 2 x 2 lambda ellipsoid (eps_r 3.0 - 0.05j, 245,760 unknowns,
+    transfer factors with the complex argument), 32 plane waves, FGMRES(50) to
+    1e-3 with inner_its near-field steps, with and without the network;
+    bistatic RCS (phi = 0, 361 angles) of 4 incidences against FP64 solves to
+    1e-6."""
+    from mlfma_pmchwt_b200 import MLFMM, learned
+    from mlfma_pmchwt_b200 import mesh as M
+    t0 = time.perf_counter()
+    train = []
+    for k, b in enumerate(M.training_ellipsoids(args.learned_bodies)):
+        op = MLFMM(b["mesh"], freq=FREQ, eps_r=b["eps_r"], leaf_coeff=0.25, device=local)
+        train.append((op, learned.random_directions(op, 32, inner_its=8, seed=k)))
+    harvest_s = time.perf_counter() - t0
+    params, hist, train_s = learned.train(train, epochs=args.learned_epochs, lr=1e-3, batch=8)
+    for op, _ in train:
+        op.close()
+    train = None
+    hb = M.held_out_ellipsoid()
+    t1 = time.perf_counter()
+    op = MLFMM(hb["mesh"], freq=FREQ, eps_r=hb["eps_r"], leaf_coeff=0.25, device=local, tf_complex_argument=True)
+    setup_s = time.perf_counter() - t1
+    inc = learned.incidences(32)
+    rhs = [op.compute_v_pmchwt(*pw) for pw in inc]
+    held = learned.random_directions(op, 8, inner_its=8, seed=999)
+    before = learned.Trainer(learned.init_params(0)).evaluate([(op, held)])
+    after = learned.Trainer(params).evaluate([(op, held)])
+    gain = learned.solve_gain(op, params, rhs, inner_its=args.inner_its, itr_max=args.solve_its)
+    # RCS of 4 incidences: near-field-preconditioned and learned solutions at
+    # 1e-3 against FP64 solves to 1e-6
+    th = np.linspace(0.0, 180.0, 361)
+    ph = np.zeros_like(th)
+    err = {"near_field": [], "learned": []}
+    for b in rhs[::8]:
+        xr, _ = op.matrix_solver(b, tol_rel=1e-6, tol_abs=0.0, mr=50, itr_max=args.solve_its, inner_its=16)
+        _, ref_db = op.calculate_rcs_pmchwt(xr, th, ph)
+        for tag, p in (("near_field", None), ("learned", params)):
+            op.attach_learned(p)
+            x, _ = op.matrix_solver(b, tol_rel=1e-3, tol_abs=0.0, mr=50, itr_max=args.solve_its,
+                                    inner_its=args.inner_its)
+            _, db = op.calculate_rcs_pmchwt(x, th, ph)
+            err[tag].append(float(np.abs(db[:, 0] - ref_db[:, 0]).max()))
+        op.attach_learned(None)
+    out = {"workload": "held-out ellipsoid 6 x 2 x 2 lambda, eps_r 3.0-0.05j, 245,760 unknowns, 32 plane waves",
+           "training": {"bodies": args.learned_bodies, "unknowns_each": 15360, "pairs": 32 * args.learned_bodies,
+                        "epochs": args.learned_epochs, "objective": "|A M v - v|^2 / |v|^2, white-noise v",
+                        "loss_first_epoch": round(hist[0], 5), "loss_last_epoch": round(hist[-1], 5),
+                        "harvest_s": round(harvest_s, 2), "train_s": round(train_s, 2)},
+           "held_out_objective": {"near_field_only": round(before["network"], 5),
+                                  "with_network": round(after["network"], 5)},
+           "setup_s": round(setup_s, 2), "inner_its": args.inner_its, "tol": 1e-3,
+           "rcs_max_db_error_vs_fp64_1e-6": {k: round(max(v), 4) for k, v in err.items()}}
+    for tag in ("near_field", "learned"):
+        g = gain[tag]
+        out[tag] = {"iterations_mean": round(g["iterations_mean"], 2), "iterations_max": max(g["iterations"]),
+                    "s_per_rhs": round(g["s_per_rhs"], 4), "converged": g["converged"]}
+    op.close()
+    return out
+
+
 def batched_apply_study(args, local: int, wl: dict) -> dict:
     """The batched complex64 apply of 16 right-hand sides on the workload's
     sphere (mixed-precision plan): per-batch CUDA-event time with the leaf
@@ -446,6 +510,10 @@ def run_product(args):
     if args.batched_only:  # the batched-apply study alone (small enough for profiler captures)
         if rank == 0:
             print(json.dumps({"batched_apply": batched_apply_study(args, local, wl)}))
+        return 0
+    if args.learned_only:  # the learned-preconditioner study alone
+        if rank == 0:
+            print(json.dumps({"learned_preconditioner": learned_study(args, local)}))
         return 0
     m = M.icosphere(wl["sub"], wl["radius"])
     t0 = time.perf_counter()
@@ -626,6 +694,8 @@ def run_product(args):
         line["multi_rhs"] = multi_rhs_study(args, local)
     if args.bodies and world == 1:
         line["uneven_bodies"] = bodies_study(args, local)
+    if args.learned and world == 1:
+        line["learned_preconditioner"] = learned_study(args, local)
     if solve:
         line["solve"] = solve
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -666,6 +736,11 @@ def main(argv=None):
                     help="skip the complex64 (mixed-precision) operator and solve")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the 16-right-hand-side batched complex64 apply study and print its record")
+    ap.add_argument("--learned", action="store_true", help="also run the learned-preconditioner study")
+    ap.add_argument("--learned-only", action="store_true", help="run only the learned-preconditioner study")
+    ap.add_argument("--learned-bodies", type=int, default=24,
+                    help="training ellipsoids of the learned-preconditioner study")
+    ap.add_argument("--learned-epochs", type=int, default=10)
     ap.add_argument("--bodies-workers", type=int, default=4,
                     help="bodies solved at once by the --bodies study (host threads, one plan each)")
     ap.add_argument("--tuning", default="auto",

@@ -286,6 +286,53 @@ MLFMA_API int mlfma_solve_mixed_batch(mlfma_plan* plan, int n, int R, double* x,
  * Code/MLFMM.cpp:353-366 without the far field). Asynchronous on stream. */
 MLFMA_API int mlfma_apply_near_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream);
 
+/* z = the near-field preconditioner of mlfma_fgmres applied to v (inner_its
+ * GMRES steps from zero on the complex64 Z_near), device vectors; returns
+ * after the result is complete. */
+MLFMA_API int mlfma_near_precondition_device(mlfma_plan* plan, int n, int inner_its, const void* v_dev,
+                                             void* z_dev, void* stream);
+
+/* Learned preconditioner (no counterpart in the reference). A message-passing
+ * network over the leaf boxes corrects the near-field preconditioner's
+ * output: y = z + sum_t G_t u_t per RWG, with linear terms u built from z
+ * (z itself and dipole projections of its box, one-ring and two-ring
+ * means) and complex gains G predicted from static geometric and material
+ * features, so that y = (I + L) z is linear. 3 layers of width 64, bfloat16
+ * weights, FP32 arithmetic; parameters are one float vector of
+ * mlfma_lp_param_count() entries (We, be, (Ws, Wn, Wg, c) x 3, Wd1, d1, Wd2,
+ * d2, row-major). Training pairs are (v, z = P_near v), with e = A^-1 v for
+ * the error loss.
+ *
+ * mlfma_lp_forward_device: y = the network's output for (v, z) with the
+ * float parameters params_dev (NULL: the attached network); y may alias z.
+ * It keeps the intermediates that mlfma_lp_backward_device needs.
+ * mlfma_lp_backward_device: after mlfma_lp_forward_device with the same
+ * parameters, adds to grad_dev the parameter gradient of any loss L(y) given
+ * gy = dL/dRe(y) + j dL/dIm(y) (complex128 [2N]), e.g. the residual-space
+ * loss |A y - v|^2 / |v|^2 with gy = 2 A^H (A y - v) / |v|^2. (v enters
+ * the network only through z; it is passed for the interface's symmetry.)
+ * mlfma_lp_loss_grad_device: y as above, and adds the loss
+ * sum |y - e|^2 / sum |e|^2 to *loss_dev and its gradient with respect to
+ * the parameters (taken at their bfloat16 values) to grad_dev.
+ * mlfma_lp_adam_device: one Adam step on params_dev (moments m_dev, v_dev,
+ * step counted from 1; the gradient is multiplied by grad_scale first).
+ * mlfma_lp_attach: the network that mlfma_fgmres, mlfma_fgmres_batch and the
+ * mixed-precision solves apply after the near-field preconditioner (host
+ * parameters; nparams = 0 detaches). All device calls are asynchronous on
+ * stream (NULL: the plan's stream). */
+MLFMA_API int mlfma_lp_param_count(void);
+MLFMA_API int mlfma_lp_forward_device(mlfma_plan* plan, int n, const float* params_dev, const void* v_dev,
+                                      const void* z_dev, void* y_dev, void* stream);
+MLFMA_API int mlfma_lp_backward_device(mlfma_plan* plan, int n, const float* params_dev, const void* gy_dev,
+                                       float* grad_dev, void* stream);
+MLFMA_API int mlfma_lp_loss_grad_device(mlfma_plan* plan, int n, const float* params_dev, const void* v_dev,
+                                        const void* z_dev, const void* e_dev, void* y_dev, float* grad_dev,
+                                        float* loss_dev, void* stream);
+MLFMA_API int mlfma_lp_adam_device(int nparams, float* params_dev, const float* grad_dev, float* m_dev, float* v_dev,
+                                   float lr, float beta1, float beta2, float eps, int step, float grad_scale,
+                                   void* stream);
+MLFMA_API int mlfma_lp_attach(mlfma_plan* plan, const float* params, int nparams);
+
 /* Plane-wave excitation vector V (complex128 [2N]) -- RHS::computeV_PMCHWT
  * (Code/Vm.h:150-203) with the incident unit vectors of EMSource::initPW
  * (Code/EMSource.cpp:34-72): kinc (propagation), einc (E polarisation),

@@ -100,6 +100,14 @@ SIGNATURES = {
     "mlfma_solve_mixed_batch": (C.c_int, [_P, C.c_int, C.c_int, _DP, _DP, C.c_int, C.c_int, C.c_double, C.c_double,
                                           C.c_int, C.c_int, C.POINTER(SolveStats)]),
     "mlfma_apply_near_device": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "mlfma_near_precondition_device": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P]),
+    "mlfma_lp_param_count": (C.c_int, []),
+    "mlfma_lp_forward_device": (C.c_int, [_P, C.c_int, _P, _P, _P, _P, _P]),
+    "mlfma_lp_backward_device": (C.c_int, [_P, C.c_int, _P, _P, _P, _P]),
+    "mlfma_lp_loss_grad_device": (C.c_int, [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "mlfma_lp_adam_device": (C.c_int, [C.c_int, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_float,
+                                       C.c_int, C.c_float, _P]),
+    "mlfma_lp_attach": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int]),
     "mlfma_rhs_pmchwt": (C.c_int, [_P, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt": (C.c_int, [_P, _DP, C.c_int, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt_noalloc": (C.c_int, [_P, _P, C.c_int, _DP, _DP, _P, _P]),
@@ -172,6 +180,22 @@ def plane_wave(pol_deg: float, theta_deg: float, phi_deg: float):
     if nh > 1e-15:
         h = h / nh
     return k, e, h
+
+
+def lp_param_count() -> int:
+    """Parameters of the learned preconditioner's network."""
+    return int(load_library().mlfma_lp_param_count())
+
+
+def lp_adam_device(nparams: int, params_ptr: int, grad_ptr: int, m_ptr: int, v_ptr: int, lr: float, step: int,
+                   beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8, grad_scale: float = 1.0,
+                   stream: int | None = None):
+    """One Adam step on device float32 parameters (moments m, v; step from 1)."""
+    rc = load_library().mlfma_lp_adam_device(int(nparams), C.c_void_p(params_ptr), C.c_void_p(grad_ptr),
+                                             C.c_void_p(m_ptr), C.c_void_p(v_ptr), lr, beta1, beta2, eps, int(step),
+                                             grad_scale, C.c_void_p(stream or 0))
+    if rc < 0:
+        raise MlfmaError(rc, load_library().mlfma_last_error().decode(errors="replace"))
 
 
 class MLFMM:
@@ -441,6 +465,47 @@ class MLFMM:
         """w = Z_near x on device pointers (the near-field rows alone)."""
         self._check(self._lib.mlfma_apply_near_device(self._h, self.n, C.c_void_p(x_ptr), C.c_void_p(w_ptr),
                                                       C.c_void_p(stream or 0)))
+
+    def near_precondition_device(self, inner_its: int, v_ptr: int, z_ptr: int, stream: int | None = None):
+        """z = the near-field preconditioner of the flexible solves applied to
+        v (device complex128 [2N]); returns when z is complete."""
+        self._check(self._lib.mlfma_near_precondition_device(self._h, self.n, int(inner_its), C.c_void_p(v_ptr),
+                                                             C.c_void_p(z_ptr), C.c_void_p(stream or 0)))
+
+    # ------------------------------------------------- learned preconditioner
+    def lp_forward_device(self, params_ptr: int | None, v_ptr: int, z_ptr: int, y_ptr: int,
+                          stream: int | None = None):
+        """y = the learned correction of z = P_near v (device complex128 [2N];
+        params: device float32 [lp_param_count()], None = the attached network)."""
+        self._check(self._lib.mlfma_lp_forward_device(self._h, self.n, C.c_void_p(params_ptr or 0),
+                                                      C.c_void_p(v_ptr), C.c_void_p(z_ptr), C.c_void_p(y_ptr),
+                                                      C.c_void_p(stream or 0)))
+
+    def lp_backward_device(self, params_ptr: int, gy_ptr: int, grad_ptr: int, stream: int | None = None):
+        """After lp_forward_device: adds the parameter gradient of a loss whose
+        gradient with respect to y is gy = dL/dRe(y) + j dL/dIm(y) to grad_ptr."""
+        self._check(self._lib.mlfma_lp_backward_device(self._h, self.n, C.c_void_p(params_ptr), C.c_void_p(gy_ptr),
+                                                       C.c_void_p(grad_ptr), C.c_void_p(stream or 0)))
+
+    def lp_loss_grad_device(self, params_ptr: int, v_ptr: int, z_ptr: int, e_ptr: int, y_ptr: int, grad_ptr: int,
+                            loss_ptr: int, stream: int | None = None):
+        """Forward pass into y, then adds sum|y - e|^2 / sum|e|^2 to the float
+        at loss_ptr and its parameter gradient to grad_ptr (device float32)."""
+        self._check(self._lib.mlfma_lp_loss_grad_device(self._h, self.n, C.c_void_p(params_ptr), C.c_void_p(v_ptr),
+                                                        C.c_void_p(z_ptr), C.c_void_p(e_ptr), C.c_void_p(y_ptr),
+                                                        C.c_void_p(grad_ptr), C.c_void_p(loss_ptr),
+                                                        C.c_void_p(stream or 0)))
+
+    def attach_learned(self, params) -> None:
+        """Use the network with these (host float32) parameters after the
+        near-field preconditioner in every flexible solve; None detaches."""
+        if params is None:
+            self._check(self._lib.mlfma_lp_attach(self._h, None, 0))
+            return
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != lp_param_count():
+            raise ValueError(f"expected {lp_param_count()} parameters")
+        self._check(self._lib.mlfma_lp_attach(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
 
     def compute_v_pmchwt(self, kinc, einc, hinc) -> np.ndarray:
         V = np.empty(self.n, dtype=np.complex128)

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/mlfma_pmchwt.h"
+#include "learned.hpp"
 #include "plan.hpp"
 #include "solver.hpp"
 
@@ -558,6 +559,108 @@ int mlfma_apply_near_device(mlfma_plan* plan, int n, const void* x_dev, void* w_
     MLFMA_CUDA(cudaSetDevice(P.device));
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
     mlfma::near_apply(P, static_cast<const double2*>(x_dev), static_cast<double2*>(w_dev), s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_near_precondition_device(mlfma_plan* plan, int n, int inner_its, const void* v_dev, void* z_dev,
+                                   void* stream) {
+  if (!plan || !plan->p || !v_dev || !z_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (v_dev == z_dev) return fail(MLFMA_ERR_ARG, "v and z must not alias");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::near_precondition(P, inner_its, static_cast<const double2*>(v_dev), static_cast<double2*>(z_dev), s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_lp_param_count(void) { return mlfma::kLpParams; }
+
+int mlfma_lp_forward_device(mlfma_plan* plan, int n, const float* params_dev, const void* v_dev, const void* z_dev,
+                            void* y_dev, void* stream) {
+  if (!plan || !plan->p || !v_dev || !z_dev || !y_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    const __nv_bfloat16* w = nullptr;
+    if (params_dev) {
+      __nv_bfloat16* ws = mlfma::lp_scratch_weights(P);
+      mlfma::lp_to_bf16(params_dev, ws, mlfma::kLpParams, s);
+      w = ws;
+    } else {
+      w = mlfma::lp_attached(P);
+      if (!w) throw std::invalid_argument("no parameters given and no network attached");
+    }
+    mlfma::lp_forward(P, w, static_cast<const double2*>(v_dev), static_cast<const double2*>(z_dev),
+                      static_cast<double2*>(y_dev), true, s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_lp_backward_device(mlfma_plan* plan, int n, const float* params_dev, const void* gy_dev, float* grad_dev,
+                             void* stream) {
+  if (!plan || !plan->p || !params_dev || !gy_dev || !grad_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    __nv_bfloat16* ws = mlfma::lp_scratch_weights(P);
+    mlfma::lp_to_bf16(params_dev, ws, mlfma::kLpParams, s);
+    mlfma::lp_backward(P, ws, nullptr, nullptr, static_cast<const double2*>(gy_dev), grad_dev, nullptr, s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_lp_loss_grad_device(mlfma_plan* plan, int n, const float* params_dev, const void* v_dev, const void* z_dev,
+                              const void* e_dev, void* y_dev, float* grad_dev, float* loss_dev, void* stream) {
+  if (!plan || !plan->p || !params_dev || !v_dev || !z_dev || !e_dev || !y_dev || !grad_dev || !loss_dev)
+    return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N) return fail(MLFMA_ERR_ARG, "n must be 2N");
+  if (y_dev == v_dev || y_dev == z_dev || y_dev == e_dev) return fail(MLFMA_ERR_ARG, "y must not alias v, z or e");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    __nv_bfloat16* ws = mlfma::lp_scratch_weights(P);
+    mlfma::lp_to_bf16(params_dev, ws, mlfma::kLpParams, s);
+    mlfma::lp_forward(P, ws, static_cast<const double2*>(v_dev), static_cast<const double2*>(z_dev),
+                      static_cast<double2*>(y_dev), true, s);
+    mlfma::lp_backward(P, ws, static_cast<const double2*>(y_dev), static_cast<const double2*>(e_dev), nullptr,
+                       grad_dev, loss_dev, s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_lp_adam_device(int nparams, float* params_dev, const float* grad_dev, float* m_dev, float* v_dev, float lr,
+                         float beta1, float beta2, float eps, int step, float grad_scale, void* stream) {
+  if (nparams <= 0 || !params_dev || !grad_dev || !m_dev || !v_dev) return fail(MLFMA_ERR_ARG, "null argument");
+  if (step < 1) return fail(MLFMA_ERR_ARG, "step counts from 1");
+  return guarded([&] {
+    mlfma::lp_adam(nparams, params_dev, grad_dev, m_dev, v_dev, lr, beta1, beta2, eps, step, grad_scale,
+                   static_cast<cudaStream_t>(stream));
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_lp_attach(mlfma_plan* plan, const float* params, int nparams) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  if (nparams != 0 && (!params || nparams != mlfma::kLpParams))
+    return fail(MLFMA_ERR_ARG, "nparams must be 0 or mlfma_lp_param_count()");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    MLFMA_CUDA(cudaSetDevice(P.device));
+    MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    mlfma::lp_attach(P, params, nparams);
     return MLFMA_OK;
   });
 }

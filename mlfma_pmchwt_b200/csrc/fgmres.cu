@@ -14,6 +14,7 @@
 #include <complex>
 
 #include "blas1.cuh"
+#include "learned.hpp"
 #include "solver.hpp"
 
 namespace mlfma {
@@ -198,6 +199,75 @@ void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s, int prec)
   MLFMA_CUDA(cudaGetLastError());
 }
 
+namespace {
+
+// z = approximate solution of Z_near z = v by inner_its GMRES steps from
+// zero, with the complex64 copy of Z_near (the outer flexible GMRES admits
+// any preconditioner; its operator and residuals stay at the solve's
+// precision). The inner Hessenberg matrix, rotations and triangular solve
+// stay on the GPU: the inner steps run without a host round trip. Buffers
+// come from the caller's Work; the reduction scratch is the caller's Ops.
+struct NearPrecond {
+  Plan& P;
+  cudaStream_t s;
+  long long n;
+  int inner_its, ldi;
+  blas1::Ops ops;
+  double2* Q = nullptr;
+  InnerDev idv{};
+  NearPrecond(Plan& P_, cudaStream_t s_, int inner, blas1::Work& g, const blas1::Ops& o)
+      : P(P_), s(s_), n(2LL * P_.N), inner_its(inner), ldi(inner + 1), ops(o) {
+    if (inner_its <= 0) return;
+    Q = g.get(static_cast<size_t>(inner_its + 1) * n);
+    idv.H = g.get(static_cast<size_t>(ldi) * inner_its);
+    idv.cs = g.get(inner_its);
+    idv.sn = g.get(inner_its);
+    idv.g = g.get(ldi);
+    idv.y = g.get(inner_its);
+    idv.h1 = g.get(ldi);
+    idv.h2 = g.get(ldi);
+    idv.hn2 = g.get(1);
+    idv.sc = reinterpret_cast<double*>(g.get(2));
+    idv.flags = reinterpret_cast<int*>(g.get(1));
+  }
+  void launch(const double2* v, double2* z) {
+    blas1::norm2<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(nullptr, v, nullptr, n, ops.part);
+    inner_begin<<<1, 1, 0, s>>>(ops.part, blas1::kBlocks, idv, inner_its);
+    scale_by<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(v, idv.sc + 2, Q, n);
+    for (int j = 0; j < inner_its; ++j) {
+      const double2* q = Q + static_cast<long long>(j) * n;
+      double2* u = Q + static_cast<long long>(j + 1) * n;
+      near_apply(P, q, u, s, 1);
+      const int nv = j + 1;
+      blas1::dots<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, u, ops.part, ops.ldp);
+      blas1::reduce<<<(nv + 63) / 64, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, nv, idv.h1);
+      blas1::project_out<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, idv.h1, u, 0, ops.part, ops.ldp);
+      blas1::dots<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, u, ops.part, ops.ldp);
+      blas1::reduce<<<(nv + 63) / 64, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, nv, idv.h2);
+      blas1::project_out<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, idv.h2, u, 1, ops.part, ops.ldp);
+      blas1::reduce<<<1, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, 1, idv.hn2);
+      inner_step<<<1, 1, 0, s>>>(idv, j, ldi);
+      scale_by<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(u, idv.sc + 1, u, n);
+    }
+    inner_end<<<1, 1, 0, s>>>(idv, ldi, inner_its);
+    blas1::combine<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, inner_its, idv.y, z, 0);
+    MLFMA_CUDA(cudaGetLastError());
+  }
+};
+
+}  // namespace
+
+void near_precondition(Plan& P, int inner_its, const double2* v, double2* z, cudaStream_t s) {
+  if (inner_its < 1 || inner_its + 1 > blas1::kMaxBasis) throw std::invalid_argument("inner_its must be in 1..63");
+  MLFMA_CUDA(cudaSetDevice(P.device));
+  blas1::Work g;
+  const int ldp = blas1::kMaxBasis + 2;
+  blas1::Ops ops{s, 2LL * P.N, g.get(static_cast<size_t>(blas1::kBlocks) * ldp), ldp, g.get(2 * ldp + 2)};
+  NearPrecond np(P, s, inner_its, g, ops);
+  np.launch(v, z);
+  MLFMA_CUDA(cudaStreamSynchronize(s));  // the work arrays are freed on return
+}
+
 bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, double tol_abs, double tol_rel,
                   int inner_its, SolveStats& st, std::vector<double>& history, int prec) {
   if (prec == 1 && P.precision != 1) throw std::invalid_argument("plan was not created with mixed precision");
@@ -221,7 +291,6 @@ bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, d
   double2* w = g.get(n);
   double2* V = g.get(static_cast<size_t>(mr + 1) * n);
   double2* Zd = inner_its > 0 ? g.get(static_cast<size_t>(mr) * n) : V;
-  double2* Q = inner_its > 0 ? g.get(static_cast<size_t>(inner_its + 1) * n) : nullptr;
   double2* y = g.get(blas1::kMaxBasis);
   blas1::Ops ops{s, n, g.get(static_cast<size_t>(blas1::kBlocks) * ldp), ldp, g.get(2 * ldp + 2)};
   MLFMA_CUDA(cudaMemcpyAsync(x, xh, n * sizeof(double2), cudaMemcpyHostToDevice, s));
@@ -242,47 +311,11 @@ bool fgmres_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, d
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return ok;
   };
-  // z = approximate solution of Z_near z = v by inner_its GMRES steps from
-  // zero, with the complex64 copy of Z_near (the outer flexible GMRES admits
-  // any preconditioner; its operator and residuals stay at the solve's
-  // precision). The inner Hessenberg matrix, rotations and triangular solve
-  // stay on the GPU: the inner steps run without a host round trip.
-  const int ldi = inner_its + 1;
-  InnerDev idv{};
-  if (inner_its > 0) {
-    idv.H = g.get(static_cast<size_t>(ldi) * inner_its);
-    idv.cs = g.get(inner_its);
-    idv.sn = g.get(inner_its);
-    idv.g = g.get(ldi);
-    idv.y = g.get(inner_its);
-    idv.h1 = g.get(ldi);
-    idv.h2 = g.get(ldi);
-    idv.hn2 = g.get(1);
-    idv.sc = reinterpret_cast<double*>(g.get(2));
-    idv.flags = reinterpret_cast<int*>(g.get(1));
-  }
+  NearPrecond np(P, s, inner_its, g, ops);
   auto precondition_launch = [&](const double2* v, double2* z) {
-    blas1::norm2<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(nullptr, v, nullptr, n, ops.part);
-    inner_begin<<<1, 1, 0, s>>>(ops.part, blas1::kBlocks, idv, inner_its);
-    scale_by<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(v, idv.sc + 2, Q, n);
-    for (int j = 0; j < inner_its; ++j) {
-      const double2* q = Q + static_cast<long long>(j) * n;
-      double2* u = Q + static_cast<long long>(j + 1) * n;
-      near_apply(P, q, u, s, 1);
-      const int nv = j + 1;
-      blas1::dots<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, u, ops.part, ops.ldp);
-      blas1::reduce<<<(nv + 63) / 64, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, nv, idv.h1);
-      blas1::project_out<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, idv.h1, u, 0, ops.part, ops.ldp);
-      blas1::dots<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, u, ops.part, ops.ldp);
-      blas1::reduce<<<(nv + 63) / 64, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, nv, idv.h2);
-      blas1::project_out<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, nv, idv.h2, u, 1, ops.part, ops.ldp);
-      blas1::reduce<<<1, 64, 0, s>>>(ops.part, blas1::kBlocks, ops.ldp, 1, idv.hn2);
-      inner_step<<<1, 1, 0, s>>>(idv, j, ldi);
-      scale_by<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(u, idv.sc + 1, u, n);
-    }
-    inner_end<<<1, 1, 0, s>>>(idv, ldi, inner_its);
-    blas1::combine<<<blas1::kBlocks, blas1::kThreads, 0, s>>>(Q, n, inner_its, idv.y, z, 0);
-    MLFMA_CUDA(cudaGetLastError());
+    np.launch(v, z);
+    // a learned correction of z, when a network is attached to the plan
+    if (const __nv_bfloat16* wl = lp_attached(P)) lp_forward(P, wl, v, z, z, false, s);
   };
   // The preconditioner's ~10 launches per inner step are captured once per
   // solve as a CUDA graph on solve-owned input / output vectors (v copied in,

@@ -18,6 +18,7 @@
 #include "blas1.cuh"
 #include "cplx.cuh"
 #include "plan.hpp"
+#include "learned.hpp"
 #include "solver.hpp"
 
 namespace mlfma {
@@ -459,6 +460,9 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
     std::vector<std::vector<C>> y(Ra);
     for (int a = 0; a < Ra; ++a) back_substitute(Hi[a], ld, gi[a], used[a], y[a]);
     ops.combine(Ra, sysd, sysref(Q, qs, 0), sysref(Zd, zs, zoff), y, false);
+    // a learned correction of each z, when a network is attached to the plan
+    if (const __nv_bfloat16* wl = lp_attached(P))
+      for (int q : list) lp_forward(P, wl, V + q * vs + voff, Zd + q * zs + zoff, Zd + q * zs + zoff, false, s);
   };
 
   const double eps = 1e-16;

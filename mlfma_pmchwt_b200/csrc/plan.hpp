@@ -154,6 +154,8 @@ struct StageProfiler {
   size_t used = 0;
 };
 
+struct LearnedWork;  // learned preconditioner tables and work arrays (learned.cu)
+
 struct Plan {
   // ---- host description
   Mesh mesh;
@@ -233,6 +235,7 @@ struct Plan {
   cudaEvent_t ev_start = nullptr, ev_near = nullptr;
   StageProfiler prof;
   std::vector<ApplyGraph> graphs;
+  std::shared_ptr<LearnedWork> lp;  // allocated on first use; its device arrays are in allocations
   size_t bytes = 0;
   std::vector<void*> allocations;
 

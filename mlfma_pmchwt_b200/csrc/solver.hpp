@@ -52,6 +52,11 @@ std::vector<char> mixed_batch_solve(Plan& P, int R, double* x, const double* rhs
 // w = Z_near x on device vectors (complex128 [2N]).
 void near_apply(Plan& P, const double2* x, double2* w, cudaStream_t s, int prec = 0);
 
+// z = the near-field preconditioner applied to v (inner_its GMRES steps from
+// zero on the complex64 Z_near, as inside fgmres_solve); device vectors,
+// synchronous.
+void near_precondition(Plan& P, int inner_its, const double2* v, double2* z, cudaStream_t s);
+
 void rhs_pmchwt(Plan& P, const double kinc[3], const double einc[3], const double hinc[3], double* V);
 
 void rcs_pmchwt(Plan& P, const double* I, int n_angles, const double* theta_deg, const double* phi_deg,

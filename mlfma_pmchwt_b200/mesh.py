@@ -254,6 +254,32 @@ def uneven_bodies(seed: int = 1, freq_hz: float = 3.0e8) -> list[dict]:
     return bodies
 
 
+def training_ellipsoids(count: int = 200, seed: int = 2, freq_hz: float = 3.0e8) -> list[dict]:
+    """Triaxial ellipsoids for training the learned preconditioner, drawn
+    from std::mt19937_64(seed) (u as in uneven_bodies): per body the semi-axes
+    (0.5 + 1.5u) lambda each, then eps_r = 2 + 4u (lossless); icosphere
+    subdivision 4 mapped onto the ellipsoid (7,680 RWGs, 15,360 unknowns)."""
+    g = _MT19937_64(seed)
+    u = lambda: (g.next() >> 11) * 2.0 ** -53
+    lam = wavelength(freq_hz)
+    out = []
+    for _ in range(count):
+        a, b, c = ((0.5 + 1.5 * u()) * lam for _ in range(3))
+        er = 2.0 + 4.0 * u()
+        out.append(dict(kind="ellipsoid", mesh=ellipsoid(4, a, b, c), params=dict(sub=4, axes=(a, b, c)),
+                        eps_r=complex(er, 0.0)))
+    return out
+
+
+def held_out_ellipsoid(sub: int = 6, freq_hz: float = 3.0e8) -> dict:
+    """The evaluation body of the learned preconditioner: a 6 x 2 x 2 lambda
+    ellipsoid (semi-axes 3, 1, 1 lambda), eps_r = 3.0 - 0.05j; subdivision 6
+    gives 122,880 RWGs (245,760 unknowns)."""
+    lam = wavelength(freq_hz)
+    return dict(kind="ellipsoid", mesh=ellipsoid(sub, 3.0 * lam, 1.0 * lam, 1.0 * lam),
+                params=dict(sub=sub, axes=(3.0 * lam, lam, lam)), eps_r=complex(3.0, -0.05))
+
+
 def _mean_edge(m: Mesh) -> float:
     p = np.asarray(m.points)
     idx = {int(i): k for k, i in enumerate(m.point_ids)}
