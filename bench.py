@@ -345,6 +345,62 @@ def multi_rhs_study(args, local: int) -> dict:
     return out
 
 
+def full_rhs_study(args, local: int) -> dict:
+    """128 incidences on the 245,760-unknown sphere (r = 5 lambda, icosphere
+    sub 6, eps_r 2.5 - 0.1j, leaf 0.25 lambda; transfer factors with the
+    complex argument, with which the solves converge on this lossy body):
+    the lockstep mixed-precision solve (batched complex64 applies with the
+    tensor-core leaf stages, near-field preconditioner, FP64 refinement) to
+    1e-3, against the plain FP64 GPU path -- GMRES(50) on the FP64 operator
+    without a preconditioner, to 1e-3 or 300 iterations -- on 4 of the
+    incidences, and single FP64 FGMRES on the same 4. Monostatic RCS of 8
+    incidences against FP64 solves to 1e-6."""
+    from mlfma_pmchwt_b200 import MLFMM, plane_wave
+    from mlfma_pmchwt_b200 import mesh as M
+    lam = M.wavelength(FREQ)
+    R = 128
+    t0 = time.perf_counter()
+    op = MLFMM(M.icosphere(6, 5.0 * lam), freq=FREQ, eps_r=2.5 - 0.1j, leaf_coeff=0.25, device=local,
+               precision="mixed", tf_complex_argument=True)
+    setup = time.perf_counter() - t0
+    th = np.array([180.0 * i / (R - 1) for i in range(R)])
+    B = np.stack([op.compute_v_pmchwt(*plane_wave(90.0 * (i % 2), th[i], 0.0)) for i in range(R)])
+    out = {"workload": f"sphere r=5 lambda, icosphere sub 6, {op.n} unknowns, eps_r 2.5-0.1j, leaf 0.25 lambda, "
+                       f"complex-argument transfer factors; {R} plane waves theta 0-180 deg, phi 0, alternating "
+                       f"polarisation", "rhs": R, "tol": 1e-3, "setup_s": round(setup, 2)}
+    t = time.perf_counter()
+    Xm, sm = op.solve_mixed_batch(B, itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.study_inner_its)
+    secs = time.perf_counter() - t
+    its = [s_["iterations"] for s_ in sm]
+    out["mixed_lockstep"] = {"s_total": round(secs, 3), "s_per_rhs": round(secs / R, 4),
+                             "converged": sum(s_["converged"] for s_ in sm),
+                             "iterations_mean": round(float(np.mean(its)), 2), "iterations_max": int(max(its)),
+                             "rel_residual_max": max(s_["rel_residual"] for s_ in sm),
+                             "inner_its": args.study_inner_its}
+    plain, fg = [], []
+    for i in (0, 37, 74, 111):
+        t = time.perf_counter()
+        _, st = op.matrix_solver(B[i], itr_max=300, mr=50, tol_abs=0.0, tol_rel=1e-3)
+        plain.append((time.perf_counter() - t, st["iterations"], st["converged"], st["rel_residual"]))
+        t = time.perf_counter()
+        _, st = op.matrix_solver(B[i], itr_max=300, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.study_inner_its)
+        fg.append((time.perf_counter() - t, st["iterations"], st["converged"], st["rel_residual"]))
+    for key, rows in (("plain_fp64_gmres", plain), ("fp64_fgmres_one_at_a_time", fg)):
+        out[key] = {"s_per_rhs": round(float(np.mean([r[0] for r in rows])), 4),
+                    "iterations": [int(r[1]) for r in rows], "converged": int(sum(r[2] for r in rows)),
+                    "rel_residual_max": float(max(r[3] for r in rows)), "incidences": 4}
+    out["speedup_per_rhs_vs_plain_fp64_gmres"] = round(out["plain_fp64_gmres"]["s_per_rhs"] /
+                                                       out["mixed_lockstep"]["s_per_rhs"], 2)
+    errs = []
+    for i in range(0, R, 16):
+        xo, _ = op.matrix_solver(B[i], itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-6, inner_its=args.study_inner_its)
+        ro = op.calculate_rcs_pmchwt(xo, th[i], 0.0)[1][0, 0]
+        errs.append(abs(op.calculate_rcs_pmchwt(Xm[i], th[i], 0.0)[1][0, 0] - ro))
+    out["monostatic_rcs_error_db_vs_fp64_1e-6"] = {"mixed_max": round(float(max(errs)), 5), "incidences": len(errs)}
+    op.close()
+    return out
+
+
 def bodies_study(args, local: int) -> dict:
     """24 uneven dielectric bodies (mesh.uneven_bodies(1): icospheres,
     ellipsoids, superellipsoids; 3,840-61,440 unknowns; lossy eps_r), 16
@@ -510,6 +566,10 @@ def run_product(args):
     if args.batched_only:  # the batched-apply study alone (small enough for profiler captures)
         if rank == 0:
             print(json.dumps({"batched_apply": batched_apply_study(args, local, wl)}))
+        return 0
+    if args.full_rhs_only:  # the 128-incidence study on the 245,760-unknown sphere alone
+        if rank == 0:
+            print(json.dumps({"multi_rhs_full": full_rhs_study(args, local)}))
         return 0
     if args.learned_only:  # the learned-preconditioner study alone
         if rank == 0:
@@ -694,6 +754,8 @@ def run_product(args):
         line["multi_rhs"] = multi_rhs_study(args, local)
     if args.bodies and world == 1:
         line["uneven_bodies"] = bodies_study(args, local)
+    if args.full_rhs and args.size == "full" and world == 1:
+        line["multi_rhs_full"] = full_rhs_study(args, local)
     if args.learned and world == 1:
         line["learned_preconditioner"] = learned_study(args, local)
     if solve:
@@ -736,6 +798,9 @@ def main(argv=None):
                     help="skip the complex64 (mixed-precision) operator and solve")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the 16-right-hand-side batched complex64 apply study and print its record")
+    ap.add_argument("--no-full-rhs", dest="full_rhs", action="store_false",
+                    help="skip the 128-incidence study on the 245,760-unknown sphere (run with --size full)")
+    ap.add_argument("--full-rhs-only", action="store_true", help="run only that study")
     ap.add_argument("--learned", action="store_true", help="also run the learned-preconditioner study")
     ap.add_argument("--learned-only", action="store_true", help="run only the learned-preconditioner study")
     ap.add_argument("--learned-bodies", type=int, default=24,
