@@ -165,3 +165,35 @@ def test_training_and_the_solve_with_the_network():
     print("held-out objective", before["network"], "->", after["network"], "iterations", gain)
     for op, _ in bodies:
         op.close()
+
+
+def test_attached_network_in_lockstep_and_mixed_solves():
+    """With a network attached, each system of the lockstep FGMRES takes the
+    single solve's steps (same iterations, same solution to rounding), the
+    lockstep mixed-precision solve reaches the FP64 tolerance, and detaching
+    restores the near-field-only iteration."""
+    from mlfma_pmchwt_b200 import MLFMM, learned
+    from mlfma_pmchwt_b200 import mesh as M
+    rng = np.random.default_rng(8)
+    th = learned.init_params(2)
+    o = learned.lp_param_count() - 32 - 32 * 64       # the output layer Wd2, d2
+    th[o:] = (0.02 * rng.normal(size=th.size - o)).astype(np.float32)
+    op = MLFMM(M.ellipsoid(3, 1.0, 0.8, 0.7), freq=FREQ, eps_r=3.0 - 0.1j, leaf_coeff=0.25, device=0,
+               precision="mixed")
+    B = np.stack([op.compute_v_pmchwt(*pw) for pw in learned.incidences(3)])
+    x0, s0 = op.matrix_solver(B[0], itr_max=300, mr=30, tol_rel=1e-6, tol_abs=0.0, inner_its=4)
+    op.attach_learned(th)
+    X, st = op.matrix_solver_batch(B, itr_max=300, mr=30, tol_rel=1e-6, tol_abs=0.0, inner_its=4)
+    for j in range(3):
+        x1, s1 = op.matrix_solver(B[j], itr_max=300, mr=30, tol_rel=1e-6, tol_abs=0.0, inner_its=4)
+        assert st[j]["converged"] and s1["converged"]
+        assert st[j]["iterations"] == s1["iterations"], (j, st[j]["iterations"], s1["iterations"])
+        assert rel(X[j], x1) < 1e-8
+    Xm, sm = op.solve_mixed_batch(B, itr_max=300, mr=30, tol_rel=1e-8, tol_abs=0.0, inner_its=4, refine_max=12)
+    assert all(s["converged"] for s in sm)
+    for j in range(3):
+        assert rel(op.apply_ax(Xm[j]), B[j]) < 1e-8
+    op.attach_learned(None)
+    x2, s2 = op.matrix_solver(B[0], itr_max=300, mr=30, tol_rel=1e-6, tol_abs=0.0, inner_its=4)
+    assert s2["iterations"] == s0["iterations"] and rel(x2, x0) < 1e-12
+    op.close()
