@@ -468,8 +468,18 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   const double eps = 1e-16;
   std::vector<int> all(R);
   for (int q = 0; q < R; ++q) all[q] = q;
-  std::vector<double> rnorm = true_residuals(all);
+  // initial residuals: r = b without an apply for the systems that start from zero
+  std::vector<int> from_x;
+  for (int q = 0; q < R; ++q) {
+    const double* xq = xh + 2 * q * n;
+    if (std::any_of(xq, xq + 2 * n, [](double v) { return v != 0.0; }))
+      from_x.push_back(q);
+    else
+      MLFMA_CUDA(cudaMemsetAsync(r + q * n, 0, n * sizeof(double2), s));
+  }
+  if (!from_x.empty()) batched_apply(from_x, sysref(x, n, 0), sysref(r, n, 0));
   set_sys(all);
+  std::vector<double> rnorm = ops.norms(R, sysd, sysref(r, n, 0), sysref(b, n, 0), sysref(r, n, 0), true);
   std::vector<double> bnorm = ops.norms(R, sysd, sysref(b, n, 0));
   std::vector<double> error(R);
   std::vector<char> conv(R, 0);
