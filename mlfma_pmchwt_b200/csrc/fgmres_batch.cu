@@ -248,6 +248,67 @@ __global__ void __launch_bounds__(128) near_batch_kernel(NearBatchArg<Z> a) {
   }
 }
 
+// The same products with one CTA per (leaf box, group of kNearBoxRB systems):
+// the box's source values are staged once in shared memory ([system][J, M]
+// [source]) and read there by every target row of the box, instead of each
+// row gathering them again from the vectors. Each row's sums are formed in
+// near_batch_kernel's order (lane-strided sources, then the warp shuffle),
+// so the results are identical.
+constexpr int kNearBoxRB = 8;
+constexpr size_t kNearBoxSmemMax = 160 * 1024;
+
+template <class Z>
+__global__ void __launch_bounds__(128) near_batch_box_kernel(NearBatchArg<Z> a) {
+  extern __shared__ __align__(16) unsigned char near_smem[];
+  Z* xsm = reinterpret_cast<Z*>(near_smem);
+  const int b = blockIdx.x;
+  const int p0 = blockIdx.y * kNearBoxRB, pn = min(kNearBoxRB, a.R - p0);
+  const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
+  const int r0 = a.leaf_ptr[b], nb = a.leaf_ptr[b + 1] - r0;
+  for (int i = threadIdx.x; i < pn * ns; i += blockDim.x) {
+    const int j = i / ns, q = i - j * ns;
+    const double2* xj = a.x.at(p0 + j, a.sys);
+    const int src = a.near_src[s0 + q];
+    xsm[(2 * j) * ns + q] = Cx<Z>::from(xj[src]);
+    xsm[(2 * j + 1) * ns + q] = Cx<Z>::from(xj[a.N + src]);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int tl = threadIdx.x >> 5; tl < nb; tl += blockDim.x / 32) {
+    const int id = a.leaf_rwg[r0 + tl];
+    const Z* Zr = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
+    Z nJ[kNearBoxRB], nM[kNearBoxRB];
+#pragma unroll
+    for (int j = 0; j < kNearBoxRB; ++j) nJ[j] = nM[j] = Cx<Z>::zero();
+    for (int q = lane; q < ns; q += 32) {
+      const Z z11 = Zr[3 * q], z12 = Zr[3 * q + 1], z22 = Zr[3 * q + 2];
+#pragma unroll
+      for (int j = 0; j < kNearBoxRB; ++j) {
+        if (j < pn) {
+          const Z xJ = xsm[(2 * j) * ns + q], xM = xsm[(2 * j + 1) * ns + q];
+          nJ[j] = cfma(z11, xJ, cfma(z12, xM, nJ[j]));
+          nM[j] = cfma(z22, xM, csub(nM[j], cmul(z12, xJ)));
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kNearBoxRB; ++j) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        nJ[j].x += __shfl_xor_sync(0xffffffffu, nJ[j].x, o);
+        nJ[j].y += __shfl_xor_sync(0xffffffffu, nJ[j].y, o);
+        nM[j].x += __shfl_xor_sync(0xffffffffu, nM[j].x, o);
+        nM[j].y += __shfl_xor_sync(0xffffffffu, nM[j].y, o);
+      }
+      if (lane == 0 && j < pn) {
+        double2* w = a.w.at(p0 + j, a.sys);
+        w[id] = Cx<Z>::to64(nJ[j]);
+        w[a.N + id] = Cx<Z>::to64(nM[j]);
+      }
+    }
+  }
+}
+
 // Upper-triangular solve of the rotated least-squares system (Code/GMRES.h:165-182).
 void back_substitute(const std::vector<C>& H, int ld, const std::vector<C>& s, int m, std::vector<C>& y) {
   const double eps = 1e-16;
@@ -409,6 +470,14 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
     // r holds A x: r = b - r in place
     return ops.norms(Ra, sysd, sysref(r, n, 0), sysref(b, n, 0), sysref(r, n, 0), true);
   };
+  // the box-staged near-field kernel's shared memory: the largest source list
+  const int nleaf = static_cast<int>(P.h_near_sptr.size()) - 1;
+  int ns_max = 0;
+  for (int bx = 0; bx < nleaf; ++bx) ns_max = std::max(ns_max, P.h_near_sptr[bx + 1] - P.h_near_sptr[bx]);
+  const size_t box_smem = static_cast<size_t>(2 * kNearBoxRB) * ns_max * sizeof(float2);
+  if (inner_its > 0 && box_smem <= kNearBoxSmemMax)
+    MLFMA_CUDA(cudaFuncSetAttribute(near_batch_box_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(box_smem)));
   // z_q = (inner_its GMRES steps on Z_near from zero) applied to v_q, q in list
   auto precondition = [&](const std::vector<int>& list, long long voff, long long zoff) {
     const int Ra = static_cast<int>(list.size());
@@ -426,13 +495,18 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
     std::vector<std::vector<C>> hcol;
     std::vector<double> hn;
     for (int j = 0; j < inner_its; ++j) {
-      const dim3 ng((P.N + 3) / 4, (Ra + kNearRB - 1) / kNearRB);
       {  // the preconditioner's near field is the complex64 copy at either precision
         NearBatchArg<float2> na{P.d_leaf_rwg,  P.d_rwg_leafbox,      P.d_leaf_ptr,
                                 P.d_near_sptr, P.d_near_src,         P.d_near_zoff,
                                 P.d_near_z32,  sysref(Q, qs, j * n), sysref(Q, qs, (j + 1) * n),
                                 sysd,          P.N,                  Ra};
-        near_batch_kernel<float2><<<ng, 128, 0, s>>>(na);
+        if (box_smem <= kNearBoxSmemMax) {
+          const dim3 ng(nleaf, (Ra + kNearBoxRB - 1) / kNearBoxRB);
+          near_batch_box_kernel<float2><<<ng, 128, box_smem, s>>>(na);
+        } else {
+          const dim3 ng((P.N + 3) / 4, (Ra + kNearRB - 1) / kNearRB);
+          near_batch_kernel<float2><<<ng, 128, 0, s>>>(na);
+        }
       }
       MLFMA_CUDA(cudaGetLastError());
       for (int q : list) st[q].near_products++;
