@@ -616,8 +616,8 @@ __global__ void lp_adam_kernel(int n, float* __restrict__ th, const float* __res
 struct LearnedWork {
   int N = 0, B = 0;
   Tabs t{};
-  double* part = nullptr;   // [3][kRedBlocks]
-  double* sums = nullptr;   // [3]: [2] = sum |e|^2
+  double* part = nullptr;   // [kRedBlocks] partial sums of |e|^2
+  double* esum = nullptr;   // sum |e|^2
   float2 *zb = nullptr, *zn = nullptr, *z2 = nullptr, *u = nullptr;
   float *a = nullptr, *q = nullptr, *dG = nullptr, *dq = nullptr, *dx = nullptr;
   float* h[kLpLayers + 1] = {};
@@ -747,8 +747,8 @@ LearnedWork& lp_work(Plan& P) {
   w->t.nb_ptr = P.upload(nb_ptr);
   w->t.nb_idx = P.upload(nb_idx);
   w->t.fs = P.upload(fs);
-  w->part = P.alloc<double>(3 * kRedBlocks);
-  w->sums = P.alloc<double>(3);
+  w->part = P.alloc<double>(kRedBlocks);
+  w->esum = P.alloc<double>(1);
   w->zb = P.alloc<float2>(6 * static_cast<size_t>(B));
   w->zn = P.alloc<float2>(6 * static_cast<size_t>(B));
   w->z2 = P.alloc<float2>(6 * static_cast<size_t>(B));
@@ -816,10 +816,10 @@ void lp_backward(Plan& P, const __nv_bfloat16* w, const double2* y, const double
   LearnedWork& W = lp_work(P);
   const int N = W.N, B = W.B;
   if (!gy) {
-    lp_sumsq_kernel<<<kRedBlocks, 256, 0, s>>>(e, 2LL * N, W.part + 2 * kRedBlocks);
-    lp_finalize_kernel<<<1, 256, 0, s>>>(W.part + 2 * kRedBlocks, kRedBlocks, 1, W.sums + 2);
+    lp_sumsq_kernel<<<kRedBlocks, 256, 0, s>>>(e, 2LL * N, W.part);
+    lp_finalize_kernel<<<1, 256, 0, s>>>(W.part, kRedBlocks, 1, W.esum);
   }
-  DecBwdArg d{W.t, w, y, e, W.sums + 2, gy, W.u, W.q, W.dG, W.dq, W.dx, gy ? nullptr : loss};
+  DecBwdArg d{W.t, w, y, e, W.esum, gy, W.u, W.q, W.dG, W.dq, W.dx, gy ? nullptr : loss};
   lp_decode_bwd_kernel<<<(N + kDecRows - 1) / kDecRows, 128, dec_bwd_smem(), s>>>(d);
   wgrad(W.dG, kLpG, kLpG, W.q, kLpH, kLpH, nullptr, N, grad + kLpOffWd2, kLpH, grad + kLpOffD2, s);
   wgrad(W.dq, kLpH, kLpH, W.h[kLpLayers], kLpH, kLpH, W.t.pos_box, N, grad + kLpOffWd1, 2 * kLpH, grad + kLpOffD1, s);
