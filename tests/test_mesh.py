@@ -68,3 +68,24 @@ def test_uneven_body_set():
     again = M.uneven_bodies(1)
     for a, b in zip(bodies, again):
         assert a["eps_r"] == b["eps_r"] and np.array_equal(a["mesh"].points, b["mesh"].points)
+
+
+def test_learned_preconditioner_body_sets():
+    """Training ellipsoids (seeded, semi-axes 0.5-2 lambda, eps_r 2-6,
+    15,360 unknowns each) and the held-out 6 x 2 x 2 lambda ellipsoid
+    (245,760 unknowns)."""
+    lam = M.wavelength(3.0e8)
+    bodies = M.training_ellipsoids(5)
+    for b in bodies:
+        assert 3 * len(b["mesh"].face_ids) == 15360
+        assert all(0.5 * lam <= a <= 2.0 * lam for a in b["params"]["axes"])
+        assert 2.0 <= b["eps_r"].real <= 6.0 and b["eps_r"].imag == 0.0
+        p = b["mesh"].points / np.asarray(b["params"]["axes"])
+        np.testing.assert_allclose(np.linalg.norm(p, axis=1), 1.0, atol=1e-12)
+    again = M.training_ellipsoids(5)
+    assert all(a["params"]["axes"] == b["params"]["axes"] and a["eps_r"] == b["eps_r"] for a, b in zip(bodies, again))
+    assert [b["params"]["axes"] for b in M.training_ellipsoids(2, seed=3)] != [b["params"]["axes"] for b in bodies[:2]]
+    h = M.held_out_ellipsoid(sub=3)
+    assert h["eps_r"] == complex(3.0, -0.05)
+    np.testing.assert_allclose(h["params"]["axes"], (3.0 * lam, lam, lam))
+    assert 3 * len(M.held_out_ellipsoid(sub=4)["mesh"].face_ids) == 15360  # 245,760 at sub 6
