@@ -203,9 +203,9 @@ class Trainer:
         self.tstream.synchronize()
         return self.theta.cpu().numpy()
 
-    def _loss_grad(self, op: MLFMM, data: dict, k: int, buf):
-        """Adds pair k's loss to self.loss and its parameter gradient to
-        self.grad. Error loss: |y - e|^2 / |e|^2. Residual loss:
+    def _loss_grad(self, op: MLFMM, data: dict, k: int, buf, grad: bool = True):
+        """Adds pair k's loss to self.loss and (grad, or always for the error
+        loss) its parameter gradient to self.grad. Error loss: |y - e|^2 / |e|^2. Residual loss:
         |A y - v|^2 / |v|^2. Aligned loss: the part of v that the direction
         A y leaves unexplained, min over complex a of |a A y - v|^2 / |v|^2
         (what one flexible GMRES step gains from y). With r = a A y - v
@@ -231,6 +231,8 @@ class Trainer:
             alpha = self.torch.ones((), dtype=w.dtype, device=w.device)
         w.sub_(v)
         self.loss.add_((torch_sq(self.torch, w) / vn2).float())
+        if not grad:
+            return
         a.copy_(w.conj())
         a[N:].neg_()
         op.apply_device(a.data_ptr(), y.data_ptr(), self.stream)
@@ -284,7 +286,7 @@ class Trainer:
             buf = self._buffers(d)
             for k in range(d["v"].shape[0]):
                 self.loss.zero_()
-                self._loss_grad(op, d, k, buf)
+                self._loss_grad(op, d, k, buf, grad=False)
                 net += float(self.loss.item())
                 v, z = d["v"][k], d["z"][k]
                 if self.loss_kind == "error":
