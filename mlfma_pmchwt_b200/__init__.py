@@ -624,4 +624,5 @@ class MLFMM:
         return dict(target=t, source=s, z11=z[0], z12=z[1], z22=z[2])
 
 
-__all__ = ["MLFMM", "Mesh", "MlfmaError", "load_library", "plane_wave", "mesh_mod", "SIGNATURES", "LIB_PATH"]
+__all__ = ["MLFMM", "Mesh", "MlfmaError", "load_library", "plane_wave", "mesh_mod", "SIGNATURES", "LIB_PATH",
+           "lp_param_count", "lp_adam_device"]

@@ -3,7 +3,6 @@ include/mlfma_pmchwt.h declares, and maps bad input onto status codes
 (no exception crosses the boundary). No compute call is made here."""
 import ctypes as C
 import re
-from pathlib import Path
 
 import numpy as np
 import pytest
