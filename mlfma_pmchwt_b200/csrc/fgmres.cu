@@ -163,8 +163,8 @@ __global__ void inner_end(InnerDev d, int ld, int inner) {
   }
 }
 
-// dst = src * s[0]
-__global__ void scale_by(const double2* __restrict__ src, const double* s, double2* __restrict__ dst, long long n) {
+// dst = src * s[0]; dst may be src (the inner step scales its vector in place)
+__global__ void scale_by(const double2* src, const double* s, double2* dst, long long n) {
   const double a = *s;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] = cscale(src[i], a);

@@ -785,8 +785,8 @@ LearnedWork& lp_work(Plan& P) {
 
 static const __nv_bfloat16* layer_w(const __nv_bfloat16* w, int l) { return w + kLpOffLayer0 + l * kLpLayerSize; }
 
-void lp_forward(Plan& P, const __nv_bfloat16* w, const double2* v, const double2* z, double2* y, bool train,
-                cudaStream_t s) {
+void lp_forward(Plan& P, const __nv_bfloat16* w, const double2* /* v: enters through z */, const double2* z,
+                double2* y, bool train, cudaStream_t s) {
   LearnedWork& W = lp_work(P);
   const int N = W.N, B = W.B;
   lp_boxz_kernel<<<(B + 127) / 128, 128, 0, s>>>(W.t, z, W.zb);
