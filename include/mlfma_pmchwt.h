@@ -69,6 +69,12 @@ typedef struct {
   int tf_complex_argument;     /* 0 (default): transfer factors with h2_l(|kR|) as the reference
                                   (Code/AlgoMLFMM.h:262-265); 1: h2_l(kR) with complex kR, a
                                   departure from the reference for lossy media */
+  int same_triangle_k;         /* near-field K entries of RWG pairs that share a triangle
+                                  (Code/Operator.h:325-707, 883-1046). 0 (default): evaluated on
+                                  the GPU at the exact height 0 of a field point above its own
+                                  triangle. 1: evaluated on the host with the reference's own
+                                  arithmetic, including its rounding-noise height n.(r - v_i),
+                                  which reproduces the reference's entries bit for bit */
 } mlfma_params;
 
 #define MLFMA_PREC_FP64 0
@@ -348,6 +354,36 @@ MLFMA_API int mlfma_rhs_pmchwt(mlfma_plan* plan, const double kinc[3], const dou
 MLFMA_API int mlfma_rcs_pmchwt(mlfma_plan* plan, const double* I, int n_angles, const double* theta_deg,
                      const double* phi_deg, double* field, double* rcs_db);
 
+/* Excitation vectors of R plane waves in one call -- RHS::computeV_PMCHWT
+ * (Code/Vm.h:150-203) per incidence, as the mono-static study calls it once
+ * per angle (Code/RCS.h:436-494). kinc/einc/hinc: host tables [R][3] (read
+ * before the call returns); V_dev: device complex128 [R][2N]. Asynchronous on
+ * `stream` (NULL = the plan's stream); allocates nothing. */
+MLFMA_API int mlfma_rhs_pmchwt_batch_device(mlfma_plan* plan, int n, int R, const double* kinc, const double* einc,
+                                            const double* hinc, void* V_dev, void* stream);
+
+/* Bistatic far field of R current vectors in one call -- RCSUtils::
+ * calculateRCS_PMCHWT (Code/RCS.h:116-192) for every (solution, angle), as
+ * the dual-static study evaluates it (Code/RCS.h:345-425). I_dev: device
+ * complex128 [R][2N]; theta_deg/phi_deg: host [n_angles] (read before the
+ * call returns); field_dev: device complex128 [R][n_angles][3] (Cartesian E).
+ * Asynchronous; allocates nothing. */
+MLFMA_API int mlfma_rcs_pmchwt_batch_device(mlfma_plan* plan, int n, int R, const void* I_dev, int n_angles,
+                                            const double* theta_deg, const double* phi_deg, void* field_dev,
+                                            void* stream);
+
+/* Monostatic far field: solution r observed at its own angle
+ * (theta_deg[r], phi_deg[r]), the backscatter evaluation of the mono-static
+ * loop (Code/RCS.h:436-494). field_dev: device complex128 [R][3]. */
+MLFMA_API int mlfma_rcs_pmchwt_mono_device(mlfma_plan* plan, int n, int R, const void* I_dev,
+                                           const double* theta_deg, const double* phi_deg, void* field_dev,
+                                           void* stream);
+
+/* RCS in dBsm from far fields (host, 6 doubles per angle): total,
+ * theta-pol and phi-pol per angle, formed as Code/RCS.h:391-410 does. */
+MLFMA_API int mlfma_rcs_db(int n_angles, const double* theta_deg, const double* phi_deg, const double* field,
+                           double* rcs_db);
+
 /* Far field without device allocation. No counterpart in the reference.
  * For callers that cannot allocate device memory while they run -- e.g. an
  * application that reserves all device memory up front in its own pool, or a
@@ -360,14 +396,21 @@ MLFMA_API int mlfma_rcs_pmchwt(mlfma_plan* plan, const double* I, int n_angles, 
  *  - n_angles <= mlfma_rcs_noalloc_max_angles() (8192); larger counts return
  *    MLFMA_ERR_ARG with a message and launch nothing.
  *  - Calls no cudaMalloc, cudaFree or allocating library routine.
- *  - The first call on a device looks up the array's device address
- *    (cudaGetSymbolAddress) with that device current; make that first call
+ *  - The first call on a device, with any n_angles (0 included), does the
+ *    set-up: it looks up the array's device address (cudaGetSymbolAddress)
+ *    with that device current and loads the kernel. Make that first call
  *    before any stream capture.
  *  - Every call shares the one array (it keeps the last call's angles):
  *    calls that overlap on the GPU, on any stream or plan, race. Order them on
  *    one stream or synchronise between them.
- *  - Asynchronous on `stream` (NULL = the plan's stream); theta_deg and
- *    phi_deg are host arrays read before the call returns. */
+ *  - Asynchronous on `stream` (NULL = the plan's stream). theta_deg and
+ *    phi_deg are host arrays copied into the device array by
+ *    cudaMemcpyAsync on that stream. From pageable memory the copy has taken
+ *    the values when the call returns (at the cost of the stream
+ *    synchronisation the runtime performs for pageable copies). From pinned
+ *    memory the copy reads them when the stream reaches it: such arrays must
+ *    stay valid and unchanged until then.
+ *  - The caller's current device is the same after the call as before. */
 MLFMA_API int mlfma_rcs_pmchwt_noalloc(mlfma_plan* plan, const void* I_dev, int n_angles,
                                        const double* theta_deg, const double* phi_deg, void* field_dev,
                                        void* stream);
@@ -405,6 +448,14 @@ MLFMA_API long long mlfma_get_transfer(mlfma_plan* plan, int medium, int level, 
  * z21 = -z12). Returns the pair count when pointers are NULL. */
 MLFMA_API long long mlfma_get_near(mlfma_plan* plan, int* target, int* source, double* z11, double* z12,
                          double* z22);
+
+/* The near pairs whose RWGs share a triangle, in the plan's near-field
+ * order: t, s (reference RWG ids) and z12 = -(K(k1) + K(k2)) evaluated on the
+ * host with the reference's own arithmetic (Code/Zmartix.h:605-612,
+ * Code/Operator.h:325-707, 883-1046), whatever the plan's same_triangle_k.
+ * Host-only plans (device < 0) answer too. Returns the pair count when the
+ * pointers are NULL. */
+MLFMA_API long long mlfma_get_near_same_triangle(mlfma_plan* plan, int* target, int* source, double* z12);
 
 /* Near (26-neighbourhood, Code/OCTree.cpp:385-426) and interaction lists
  * (Code/OCTree.cpp:428-488) of a level in CSR form over the plan's box

@@ -46,7 +46,7 @@ class Params(C.Structure):
     _fields_ = [("freq_hz", C.c_double), ("eps_r_re", C.c_double), ("eps_r_im", C.c_double),
                 ("mu_r_re", C.c_double), ("mu_r_im", C.c_double), ("leaf_coeff", C.c_double),
                 ("gauss_points", C.c_int), ("precision", C.c_int), ("device", C.c_int), ("verbose", C.c_int),
-                ("tf_complex_argument", C.c_int)]
+                ("tf_complex_argument", C.c_int), ("same_triangle_k", C.c_int)]
 
 
 class Info(C.Structure):
@@ -122,6 +122,7 @@ SIGNATURES = {
     "mlfma_get_pattern": (C.c_longlong, [_P, C.c_int, C.c_int, _DP]),
     "mlfma_get_transfer": (C.c_longlong, [_P, C.c_int, C.c_int, _IP, _DP]),
     "mlfma_get_near": (C.c_longlong, [_P, _IP, _IP, _DP, _DP, _DP]),
+    "mlfma_get_near_same_triangle": (C.c_longlong, [_P, _IP, _IP, _DP]),
 }
 
 _lib = None
@@ -214,7 +215,7 @@ class MLFMM:
     def __init__(self, mesh: Mesh | None = None, *, nas_path: str | None = None, freq: float = 3.0e8,
                  eps_r: complex = 4.0, mu_r: complex = 1.0, leaf_coeff: float = 0.3, gauss_points: int = 7,
                  device: int = 0, verbose: bool = False, tf_complex_argument: bool = False,
-                 precision: str = "fp64"):
+                 precision: str = "fp64", same_triangle_k: str = "exact"):
         self._lib = load_library()
         prm = Params()
         self._lib.mlfma_default_params(C.byref(prm))
@@ -223,6 +224,9 @@ class MLFMM:
         prm.mu_r_re, prm.mu_r_im = mu_r.real, mu_r.imag
         prm.leaf_coeff, prm.gauss_points, prm.device, prm.verbose = leaf_coeff, gauss_points, device, int(verbose)
         prm.tf_complex_argument = int(tf_complex_argument)
+        if same_triangle_k not in ("exact", "reference"):
+            raise ValueError("same_triangle_k must be 'exact' or 'reference'")
+        prm.same_triangle_k = 1 if same_triangle_k == "reference" else 0
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         prm.precision = 1 if precision == "mixed" else 0
@@ -622,6 +626,17 @@ class MLFMM:
         z = [np.empty(cnt, dtype=np.complex128) for _ in range(3)]
         self._check(self._lib.mlfma_get_near(self._h, _ip(t), _ip(s), *(_dp(v.view(np.float64)) for v in z)))
         return dict(target=t, source=s, z11=z[0], z12=z[1], z22=z[2])
+
+    def near_same_triangle(self) -> dict:
+        """The near pairs whose RWGs share a triangle, in the plan's order, with
+        z12 evaluated on the host with the reference's own arithmetic (works on
+        host-only plans)."""
+        cnt = self._check(self._lib.mlfma_get_near_same_triangle(self._h, None, None, None))
+        t = np.empty(cnt, dtype=np.int32)
+        s = np.empty(cnt, dtype=np.int32)
+        z = np.empty(cnt, dtype=np.complex128)
+        self._check(self._lib.mlfma_get_near_same_triangle(self._h, _ip(t), _ip(s), _dp(z.view(np.float64))))
+        return dict(target=t, source=s, z12=z)
 
 
 __all__ = ["MLFMM", "Mesh", "MlfmaError", "load_library", "plane_wave", "mesh_mod", "SIGNATURES", "LIB_PATH",

@@ -11,6 +11,7 @@
 
 #include "../../include/mlfma_pmchwt.h"
 #include "learned.hpp"
+#include "near_same_triangle.hpp"
 #include "plan.hpp"
 #include "solver.hpp"
 
@@ -56,6 +57,7 @@ mlfma::PlanParams to_params(const mlfma_params* p) {
   q.device = p->device;
   q.verbose = p->verbose;
   q.tf_complex_argument = p->tf_complex_argument;
+  q.same_triangle_k = p->same_triangle_k;
   q.precision = p->precision == MLFMA_PREC_MIXED ? 1 : 0;
   return q;
 }
@@ -705,6 +707,56 @@ int mlfma_rcs_pmchwt_noalloc(mlfma_plan* plan, const void* I_dev, int n_angles, 
 
 int mlfma_rcs_noalloc_max_angles(void) { return mlfma::rcs_noalloc_max_angles(); }
 
+int mlfma_rhs_pmchwt_batch_device(mlfma_plan* plan, int n, int R, const double* kinc, const double* einc,
+                                  const double* hinc, void* V_dev, void* stream) {
+  if (!plan || !plan->p || (R > 0 && (!kinc || !einc || !hinc || !V_dev))) return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N || R < 0) return fail(MLFMA_ERR_ARG, "n must be 2N and R >= 0");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::rhs_pmchwt_batch(P, R, kinc, einc, hinc, static_cast<double2*>(V_dev), s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_rcs_pmchwt_batch_device(mlfma_plan* plan, int n, int R, const void* I_dev, int n_angles,
+                                  const double* theta_deg, const double* phi_deg, void* field_dev, void* stream) {
+  if (!plan || !plan->p || (R > 0 && n_angles > 0 && (!I_dev || !theta_deg || !phi_deg || !field_dev)))
+    return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N || R < 0 || n_angles < 0) return fail(MLFMA_ERR_ARG, "n must be 2N, R and n_angles >= 0");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::rcs_pmchwt_batch(P, R, static_cast<const double2*>(I_dev), n_angles, theta_deg, phi_deg,
+                            static_cast<double2*>(field_dev), s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_rcs_pmchwt_mono_device(mlfma_plan* plan, int n, int R, const void* I_dev, const double* theta_deg,
+                                 const double* phi_deg, void* field_dev, void* stream) {
+  if (!plan || !plan->p || (R > 0 && (!I_dev || !theta_deg || !phi_deg || !field_dev)))
+    return fail(MLFMA_ERR_ARG, "null argument");
+  if (n != 2 * plan->p->N || R < 0) return fail(MLFMA_ERR_ARG, "n must be 2N and R >= 0");
+  if (!device_plan(plan)) return fail(MLFMA_ERR_UNSUPPORTED, "plan has no device operator");
+  return guarded([&] {
+    mlfma::Plan& P = *plan->p;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
+    mlfma::rcs_pmchwt_mono(P, R, static_cast<const double2*>(I_dev), theta_deg, phi_deg,
+                           static_cast<double2*>(field_dev), s);
+    return MLFMA_OK;
+  });
+}
+
+int mlfma_rcs_db(int n_angles, const double* theta_deg, const double* phi_deg, const double* field, double* rcs_db) {
+  if (n_angles < 0 || (n_angles > 0 && (!theta_deg || !phi_deg || !field || !rcs_db)))
+    return fail(MLFMA_ERR_ARG, "null argument or negative count");
+  mlfma::rcs_db(n_angles, theta_deg, phi_deg, field, rcs_db);
+  return MLFMA_OK;
+}
+
 int mlfma_get_rwgs(const mlfma_plan* plan, int* face_pos, int* face_neg, int* free_pos, int* free_neg,
                    int* edge_a, int* edge_b, double* length, double* mid) {
   if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
@@ -902,6 +954,32 @@ long long mlfma_get_near(mlfma_plan* plan, int* target, int* source, double* z11
     return 0;
   });
   return st == 0 ? P.near_pairs : st;
+}
+
+long long mlfma_get_near_same_triangle(mlfma_plan* plan, int* target, int* source, double* z12) {
+  if (!plan || !plan->p) return fail(MLFMA_ERR_ARG, "null plan");
+  mlfma::Plan& P = *plan->p;
+  long long count = 0;
+  int st = guarded([&] {
+    std::vector<long long> pos;
+    std::vector<int> tgt, src;
+    mlfma::same_triangle_pairs(P.rwg, P.tree, P.h_near_sptr, P.h_near_src, P.h_near_zoff, pos, tgt, src);
+    count = static_cast<long long>(pos.size());
+    for (long long i = 0; i < count; ++i) {
+      if (target) target[i] = tgt[i];
+      if (source) source[i] = src[i];
+    }
+    if (z12) {
+      std::vector<mlfma::cplx> z;
+      mlfma::same_triangle_z12(P.mesh, P.rwg, P.quad, P.k1, P.k2, tgt, src, z);
+      for (long long i = 0; i < count; ++i) {
+        z12[2 * i] = z[i].real();
+        z12[2 * i + 1] = z[i].imag();
+      }
+    }
+    return 0;
+  });
+  return st == 0 ? count : st;
 }
 
 }  // extern "C"

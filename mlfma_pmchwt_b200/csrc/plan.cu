@@ -7,6 +7,7 @@
 #include <map>
 
 #include "cplx.cuh"
+#include "near_same_triangle.hpp"
 #include "plan.hpp"
 
 namespace mlfma {
@@ -83,6 +84,9 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
   P->device = prm.device;
   P->verbose = prm.verbose;
   P->tf_complex_argument = prm.tf_complex_argument;
+  if (prm.same_triangle_k != 0 && prm.same_triangle_k != 1)
+    throw std::invalid_argument("same_triangle_k must be 0 (exact height) or 1 (the reference's arithmetic)");
+  P->same_triangle_k = prm.same_triangle_k;
   if (prm.precision != 0 && prm.precision != 1) throw std::invalid_argument("precision must be 0 (FP64) or 1 (mixed)");
   P->precision = prm.precision;
   P->mesh = std::move(mesh);
@@ -485,6 +489,22 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
     P->d_near_zoff = P->upload(P->h_near_zoff);
     P->d_near_z = P->alloc<double2>(3 * static_cast<size_t>(std::max<long long>(P->near_pairs, 1)));
     launch_near(*P, s);
+    if (P->same_triangle_k == 1) {
+      // the K entries of RWG pairs sharing a triangle, with the reference's
+      // arithmetic on the host, written over the device kernel's
+      std::vector<long long> pos;
+      std::vector<int> tgt, src;
+      same_triangle_pairs(P->rwg, P->tree, P->h_near_sptr, P->h_near_src, P->h_near_zoff, pos, tgt, src);
+      std::vector<cplx> z12;
+      same_triangle_z12(P->mesh, P->rwg, P->quad, P->k1, P->k2, tgt, src, z12);
+      const long long n = static_cast<long long>(pos.size());
+      P->same_triangle_pairs = n;
+      if (n > 0) {
+        std::vector<double2> zv(z12.size());
+        for (size_t i = 0; i < z12.size(); ++i) zv[i] = make_double2(z12[i].real(), z12[i].imag());
+        launch_near_z12_scatter(P->d_near_z, P->upload(pos), P->upload(zv), n, s);
+      }
+    }
   }
   P->d_x = P->alloc<double2>(2 * static_cast<size_t>(P->N));
   P->d_w = P->alloc<double2>(2 * static_cast<size_t>(P->N));

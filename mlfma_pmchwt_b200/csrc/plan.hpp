@@ -167,6 +167,8 @@ struct Plan {
   int device = 0;
   int verbose = 0;
   int tf_complex_argument = 0;
+  int same_triangle_k = 0;          // PlanParams::same_triangle_k
+  long long same_triangle_pairs = 0;  // pairs whose z12 the host evaluated (same_triangle_k = 1)
   int precision = 0;                // 0: FP64 operator; 1: also the complex64 operator
   cplx k1, k2, eta1, eta2, etai, epsr, mur;
   double lambda = 0.0, freq = 0.0;
@@ -281,6 +283,12 @@ struct PlanParams {
   // lossy (complex) k (Code/AlgoMLFMM.h:262-265). 1: h2_l(kR) with the
   // complex argument, consistent with the complex-k shifts and near field.
   int tf_complex_argument = 0;
+  // 0: near-field K entries of RWG pairs sharing a triangle at the exact
+  // height 0 of a field point above its own triangle (device kernel). 1: those
+  // entries evaluated on the host with the reference's own arithmetic, which
+  // reproduces its rounding-noise height n.(r - v_i) (Code/Operator.h:582-652)
+  // and so its entries bit for bit.
+  int same_triangle_k = 0;
   // 0: FP64 operator only. 1: also complex64 copies of the patterns, transfer
   // factors, shift phases, near field and workspaces, for the mixed-precision
   // apply and solves.
@@ -325,6 +333,8 @@ void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& 
                      const std::vector<int>& hoff, const std::vector<int>& hL,
                      const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s);
 void launch_near(Plan& P, cudaStream_t s);
+// Z[3 pos[i] + 1] = z12[i] for n entries of the near field (device arrays).
+void launch_near_z12_scatter(double2* Z, const long long* pos, const double2* z12, long long n, cudaStream_t s);
 void apply_device(Plan& P, const double2* x, double2* w, cudaStream_t s);
 void clear_graphs(Plan& P);  // after any change that alters what an apply launches
 // Batched apply: W[j] = A X[j] for j < R; X[j] at X + j * ldx (ldx >= 2N),

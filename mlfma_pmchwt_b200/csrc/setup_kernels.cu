@@ -487,6 +487,18 @@ void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& 
   cudaFree(d_wth);
 }
 
+__global__ void near_z12_scatter_kernel(double2* __restrict__ Z, const long long* __restrict__ pos,
+                                        const double2* __restrict__ z12, long long n) {
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i < n) Z[3 * pos[i] + 1] = z12[i];
+}
+
+void launch_near_z12_scatter(double2* Z, const long long* pos, const double2* z12, long long n, cudaStream_t s) {
+  if (n <= 0) return;
+  near_z12_scatter_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(Z, pos, z12, n);
+  MLFMA_CUDA(cudaGetLastError());
+}
+
 void launch_near(Plan& P, cudaStream_t s) {
   const int B = P.lv[P.maxL].B;
   near_kernel<<<B, 128, 0, s>>>(geom_arg(P), quad_arg(P.quad), P.d_leaf_ptr, P.d_leaf_rwg, P.d_near_sptr,

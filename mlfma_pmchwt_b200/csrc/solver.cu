@@ -555,16 +555,40 @@ static __device__ __align__(256) double g_rcs_angle_scratch[2 * kNoAllocMaxAngle
 double* g_rcs_scratch_addr[64] = {nullptr};
 std::mutex g_rcs_scratch_mutex;
 
+__global__ void __launch_bounds__(256) rcs_angles_kernel(RcsArg a, const double* __restrict__ angles, int max_angles,
+                                                         const double2* __restrict__ I, double2* __restrict__ out);
+
+// Set-up on the first call on a device (that device current): the address,
+// and the kernel's function attributes, which makes a lazily loading runtime
+// load the kernel now rather than at the first launch with angles.
 double* rcs_scratch_address(int device) {
   if (device < 0 || device >= 64) throw std::invalid_argument("device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_rcs_scratch_mutex);
   if (!g_rcs_scratch_addr[device]) {
     void* p = nullptr;
     MLFMA_CUDA(cudaGetSymbolAddress(&p, g_rcs_angle_scratch));
+    cudaFuncAttributes fa{};
+    MLFMA_CUDA(cudaFuncGetAttributes(&fa, rcs_angles_kernel));
     g_rcs_scratch_addr[device] = static_cast<double*>(p);
   }
   return g_rcs_scratch_addr[device];
 }
+
+// Makes a device current for the lifetime of the object and gives the
+// caller's current device back afterwards.
+class CurrentDevice {
+ public:
+  explicit CurrentDevice(int device) {
+    MLFMA_CUDA(cudaGetDevice(&prev_));
+    if (prev_ != device) MLFMA_CUDA(cudaSetDevice(device));
+  }
+  ~CurrentDevice() { cudaSetDevice(prev_); }
+  CurrentDevice(const CurrentDevice&) = delete;
+  CurrentDevice& operator=(const CurrentDevice&) = delete;
+
+ private:
+  int prev_ = 0;
+};
 
 // Same accumulation as rcs_kernel; the direction of block b is formed from
 // the angles held in the scratch array.
@@ -625,7 +649,7 @@ void rcs_pmchwt_noalloc(Plan& P, const double2* I_dev, int n_angles, const doubl
   if (n_angles < 0 || n_angles > kNoAllocMaxAngles)
     throw std::invalid_argument("n_angles must be between 0 and " + std::to_string(kNoAllocMaxAngles) +
                                 " (size of the fixed angle scratch)");
-  MLFMA_CUDA(cudaSetDevice(P.device));
+  CurrentDevice current(P.device);
   double* scratch = rcs_scratch_address(P.device);
   if (n_angles == 0) return;
   MLFMA_CUDA(cudaMemcpyAsync(scratch, theta_deg, n_angles * sizeof(double), cudaMemcpyHostToDevice, s));

@@ -69,4 +69,19 @@ void rcs_pmchwt_noalloc(Plan& P, const double2* I_dev, int n_angles, const doubl
                         const double* phi_deg, double2* field_dev, cudaStream_t s);
 int rcs_noalloc_max_angles();
 
+// Many incidences at once (excitation.cu): the excitation vectors of R plane
+// waves (host tables [R][3]) into V_dev [R][2N]; the far field of R current
+// vectors I_dev [R][2N] at n_angles directions into field_dev
+// [R][n_angles][3] (bistatic) or each at its own direction into [R][3]
+// (monostatic). Asynchronous on s; the host tables are read at launch.
+void rhs_pmchwt_batch(Plan& P, int R, const double* kinc, const double* einc, const double* hinc, double2* V_dev,
+                      cudaStream_t s);
+void rcs_pmchwt_batch(Plan& P, int R, const double2* I_dev, int n_angles, const double* theta_deg,
+                      const double* phi_deg, double2* field_dev, cudaStream_t s);
+void rcs_pmchwt_mono(Plan& P, int R, const double2* I_dev, const double* theta_deg, const double* phi_deg,
+                     double2* field_dev, cudaStream_t s);
+// dB of far fields (6 doubles per angle) as the reference forms them:
+// total, theta-pol, phi-pol per angle.
+void rcs_db(int n_angles, const double* theta_deg, const double* phi_deg, const double* field, double* out);
+
 }  // namespace mlfma

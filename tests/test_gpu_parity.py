@@ -20,12 +20,13 @@ TABLE_TOL = 1e-11
 _ops = {}
 
 
-def gpu_op(case_files, name):
+def gpu_op(case_files, name, same_triangle_k="exact"):
     from mlfma_pmchwt_b200 import MLFMM
-    if name not in _ops:
+    key = (name, same_triangle_k)
+    if key not in _ops:
         m, p, eps, leaf = case_files[name]
-        _ops[name] = MLFMM(m, freq=FREQ, eps_r=eps, leaf_coeff=leaf, device=0)
-    return _ops[name]
+        _ops[key] = MLFMM(m, freq=FREQ, eps_r=eps, leaf_coeff=leaf, device=0, same_triangle_k=same_triangle_k)
+    return _ops[key]
 
 
 CASES = ["sphere_s2", "sphere_s3", "sphere_s3_lossy", "ellipsoid_s3", "sphere_s4_deep", "ellipsoid_s4_deep",
@@ -105,6 +106,36 @@ def test_matvec_matches_reference(case_files, ref_ops, name):
     assert rel(op.apply_ax(y), ref.apply(y)) < MATVEC_TOL
     ones = np.ones(op.n, dtype=complex)
     assert rel(op.apply_ax(ones), ref.apply(ones)) < MATVEC_TOL
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_reference_mode_matvec_matches_reference(case_files, ref_ops, name):
+    """With same_triangle_k = 'reference' (the same-triangle K entries from
+    the reference's own host arithmetic) the raw matvec matches on every
+    body, the deep ellipsoid included."""
+    from mlfma_pmchwt_b200 import mesh as M
+    op, ref = gpu_op(case_files, name, "reference"), ref_ops(name)
+    x = M.unit_disk_vector(op.n, 0)
+    err = rel(op.apply_ax(x), ref.apply(x))
+    assert err < MATVEC_TOL, err
+    ones = np.ones(op.n, dtype=complex)
+    assert rel(op.apply_ax(ones), ref.apply(ones)) < MATVEC_TOL
+
+
+@pytest.mark.parametrize("name", ["ellipsoid_s4_deep", "sphere_s3"])
+def test_reference_mode_near_field_entries(case_files, ref_ops, name):
+    """Reference mode: every near-field entry within table tolerance, and the
+    same-triangle z12 entries equal to the reference's bit for bit."""
+    op, ref = gpu_op(case_files, name, "reference"), ref_ops(name)
+    got, want, pairs = _dense_near(op, ref)
+    assert rel(got, want) < TABLE_TOL
+    scale = np.abs(want).max()
+    assert not (np.abs(got - want) > TABLE_TOL * scale).any()
+    st = op.near_same_triangle()
+    where = {(int(t), int(s)): i for i, (t, s) in enumerate(pairs)}
+    sel = np.array([where[(int(t), int(s))] for t, s in zip(st["target"], st["source"])])
+    np.testing.assert_array_equal(got[sel, 1], want[sel, 1])
+    np.testing.assert_array_equal(got[sel, 2], want[sel, 2])
 
 
 def test_same_triangle_k_terms_where_the_reference_is_ill_conditioned(case_files, ref_ops):

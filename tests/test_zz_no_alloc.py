@@ -18,8 +18,9 @@ pytestmark = [pytest.mark.gpu, needs_lib]
 def _field_noalloc(op, I, th, ph):
     import torch
     Id = torch.from_numpy(np.ascontiguousarray(I)).cuda()
-    out = torch.zeros((len(th), 3), dtype=torch.complex128, device="cuda")
+    out = torch.empty((len(th), 3), dtype=torch.complex128, device="cuda")  # every element is written
     stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())  # the copy of I_dev comes first
     op.calculate_rcs_noalloc(Id.data_ptr(), th, ph, out.data_ptr(), stream.cuda_stream)
     stream.synchronize()
     return out.cpu().numpy()
@@ -30,6 +31,14 @@ def test_noalloc_far_field_matches_allocating_entry_point():
     from mlfma_pmchwt_b200 import mesh as M
     op = MLFMM(M.icosphere(3, 1.0), freq=FREQ, eps_r=4.0, leaf_coeff=0.25, device=0)
     I = M.unit_disk_vector(op.n, 4)
+    # a first call with no angles does the per-device set-up and leaves the current device alone
+    import torch
+    dev = torch.cuda.current_device()
+    Id = torch.from_numpy(I).cuda()
+    out = torch.empty((1, 3), dtype=torch.complex128, device="cuda")
+    op.calculate_rcs_noalloc(Id.data_ptr(), np.zeros(0), np.zeros(0), out.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.cuda.current_device() == dev
     # first call: the 361-angle bistatic cut in phi = 0
     th1 = np.arange(0.0, 180.01, 0.5)
     f_ref1, _ = op.calculate_rcs_pmchwt(I, th1, 0.0)
