@@ -238,6 +238,48 @@ def cpu_baseline_reference(args, wl, rank: int) -> dict | None:
             "setup_s": setup}
 
 
+def cpu_solve_baseline(args, local: int) -> dict | None:
+    """The reference's own GMRES solve (MLFMM::matrix_solver -> MGMRES::mgmres,
+    Code/GMRES.h:65-217, OpenMP matvecs) on the 3,840-unknown sphere (radius
+    1 m, icosphere sub 3, eps_r 4, leaf 0.25 lambda; plane wave along -z,
+    x-polarised): GMRES(30) to 1e-3, bounded at --cpu-solve-its iterations
+    (it does not converge without a preconditioner). Beside it, the same
+    GMRES(30) on the GPU with the same cap, and the GPU's FGMRES with the
+    near-field preconditioner to convergence."""
+    from oracle import oracle as O
+    if not O.ref_available() or args.cpu_solve_its <= 0:
+        return None
+    from mlfma_pmchwt_b200 import MLFMM, plane_wave
+    from mlfma_pmchwt_b200 import mesh as M
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    m = M.icosphere(3, 1.0)
+    nas = M.write_nas(m, Path("/tmp") / f"bench_solve_{os.getpid()}.nas")
+    ref = O.RefOperator(nas, freq=FREQ, eps_r=4.0, leaf_coeff=0.25)
+    V = ref.rhs(0.0, 0.0, 0.0)[0]
+    its = args.cpu_solve_its
+    t = time.perf_counter()
+    _, info = ref.solve(V, itr_max=its, mr=30, tol_abs=0.0, tol_rel=1e-3)
+    ref_s = time.perf_counter() - t
+    ref.close()
+    true_r = info.get("true_residuals") or [float("nan")]
+    op = MLFMM(m, freq=FREQ, eps_r=4.0, leaf_coeff=0.25, device=local)
+    op.matrix_solver(V, itr_max=30, mr=30, tol_abs=0.0, tol_rel=1e-3)  # warm-up (graph capture)
+    _, sg = op.matrix_solver(V, itr_max=its, mr=30, tol_abs=0.0, tol_rel=1e-3)
+    _, sf = op.matrix_solver(V, itr_max=its, mr=30, tol_abs=0.0, tol_rel=1e-3, inner_its=8)
+    op.close()
+    return {"workload": "sphere r=1 m, icosphere sub 3, 3,840 unknowns, eps_r 4, leaf 0.25 lambda; plane wave "
+                        "along -z, x-polarised", "cores": cores, "kind": "reference",
+            "reference_gmres30": {"seconds": round(ref_s, 3), "iterations": len(info.get("history", [])),
+                                  "s_per_iteration": round(ref_s / max(len(info.get("history", [])), 1), 5),
+                                  "rel_residual": float(true_r[-1]), "tol": 1e-3, "itr_max": its},
+            "gpu_gmres30": {"seconds": round(sg["seconds"], 4), "iterations": sg["iterations"],
+                            "s_per_iteration": round(sg["seconds"] / max(sg["iterations"], 1), 6),
+                            "rel_residual": sg["rel_residual"], "converged": sg["converged"]},
+            "gpu_fgmres30_near8": {"seconds": round(sf["seconds"], 4), "iterations": sf["iterations"],
+                                   "rel_residual": sf["rel_residual"], "converged": sf["converged"]}}
+
+
 def run_reference_arm(args):
     # the reference's CPU matvec runs on rank 0 alone; no collective is needed
     if int(os.environ.get("RANK", "0")) != 0:
@@ -353,7 +395,9 @@ def full_rhs_study(args, local: int) -> dict:
     1e-3, against the plain FP64 GPU path -- GMRES(50) on the FP64 operator
     without a preconditioner, to 1e-3 or 300 iterations -- on 4 of the
     incidences, and single FP64 FGMRES on the same 4. Monostatic RCS of 8
-    incidences against FP64 solves to 1e-6."""
+    incidences and their bistatic RCS (phi = 0, 361 angles) against FP64
+    solves to 1e-6. The excitations come from one batched launch, the far
+    fields from the batched bistatic and monostatic kernels."""
     from mlfma_pmchwt_b200 import MLFMM, plane_wave
     from mlfma_pmchwt_b200 import mesh as M
     lam = M.wavelength(FREQ)
@@ -363,7 +407,12 @@ def full_rhs_study(args, local: int) -> dict:
                precision="mixed", tf_complex_argument=True)
     setup = time.perf_counter() - t0
     th = np.array([180.0 * i / (R - 1) for i in range(R)])
-    B = np.stack([op.compute_v_pmchwt(*plane_wave(90.0 * (i % 2), th[i], 0.0)) for i in range(R)])
+    import torch
+    Bd = torch.empty((R, op.n), dtype=torch.complex128, device=f"cuda:{local}")
+    op.compute_v_pmchwt_batch_device([plane_wave(90.0 * (i % 2), th[i], 0.0) for i in range(R)], Bd.data_ptr())
+    torch.cuda.synchronize(local)
+    B = Bd.cpu().numpy()
+    del Bd
     out = {"workload": f"sphere r=5 lambda, icosphere sub 6, {op.n} unknowns, eps_r 2.5-0.1j, leaf 0.25 lambda, "
                        f"complex-argument transfer factors; {R} plane waves theta 0-180 deg, phi 0, alternating "
                        f"polarisation", "rhs": R, "tol": 1e-3, "setup_s": round(setup, 2)}
@@ -390,14 +439,48 @@ def full_rhs_study(args, local: int) -> dict:
                     "rel_residual_max": float(max(r[3] for r in rows)), "incidences": 4}
     out["speedup_per_rhs_vs_plain_fp64_gmres"] = round(out["plain_fp64_gmres"]["s_per_rhs"] /
                                                        out["mixed_lockstep"]["s_per_rhs"], 2)
-    errs = []
-    for i in range(0, R, 16):
-        xo, _ = op.matrix_solver(B[i], itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-6, inner_its=args.study_inner_its)
-        ro = op.calculate_rcs_pmchwt(xo, th[i], 0.0)[1][0, 0]
-        errs.append(abs(op.calculate_rcs_pmchwt(Xm[i], th[i], 0.0)[1][0, 0] - ro))
-    out["monostatic_rcs_error_db_vs_fp64_1e-6"] = {"mixed_max": round(float(max(errs)), 5), "incidences": len(errs)}
+    sel = list(range(0, R, 16))
+    Xo = np.stack([op.matrix_solver(B[i], itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-6,
+                                    inner_its=args.study_inner_its)[0] for i in sel])
+    out.update(rcs_errors(op, local, Xm[sel], Xo, th[sel]))
     op.close()
     return out
+
+
+def rcs_errors(op, local: int, X, Xo, th_inc) -> dict:
+    """RCS errors (dB) of solutions X against oracle solutions Xo: monostatic
+    (backscatter at (theta_i, 0)) and bistatic (phi = 0, theta 0:0.5:180,
+    361 angles, total RCS), through the batched far-field kernels."""
+    import torch
+    from mlfma_pmchwt_b200 import rcs_db
+    R = len(X)
+    dev = f"cuda:{local}"
+    th = np.arange(0.0, 180.01, 0.5)
+    ph = np.zeros_like(th)
+    res = {}
+    for key, V in (("x", X), ("o", Xo)):
+        Vd = torch.from_numpy(np.ascontiguousarray(V)).to(dev)
+        Fb = torch.empty((R, len(th), 3), dtype=torch.complex128, device=dev)
+        Fm = torch.empty((R, 3), dtype=torch.complex128, device=dev)
+        s = torch.cuda.current_stream(local).cuda_stream
+        op.calculate_rcs_batch_device(R, Vd.data_ptr(), th, ph, Fb.data_ptr(), s)
+        op.calculate_rcs_mono_device(R, Vd.data_ptr(), th_inc, np.zeros(R), Fm.data_ptr(), s)
+        torch.cuda.synchronize(local)
+        fb, fm = Fb.cpu().numpy(), Fm.cpu().numpy()
+        res[key] = (np.stack([rcs_db(th, ph, fb[r])[:, 0] for r in range(R)]),
+                    np.array([rcs_db(th_inc[r], 0.0, fm[r:r + 1])[0, 0] for r in range(R)]))
+    bi = np.abs(res["x"][0] - res["o"][0])
+    mono = np.abs(res["x"][1] - res["o"][1])
+    # angles within 20 dB of the cut's peak (away from the deep nulls)
+    lit = res["o"][0] >= res["o"][0].max(axis=1, keepdims=True) - 20.0
+    return {"monostatic_rcs_error_db_vs_fp64_1e-6": {"mixed_max": round(float(mono.max()), 5),
+                                                      "mixed_median": round(float(np.median(mono)), 5),
+                                                      "incidences": R},
+            "bistatic_rcs_error_db_vs_fp64_1e-6": {"max": round(float(bi.max()), 5),
+                                                    "median": round(float(np.median(bi)), 5),
+                                                    "max_within_20db_of_peak": round(float(bi[lit].max()), 5),
+                                                    "angles": len(th), "incidences": R,
+                                                    "cut": "phi = 0, theta 0:0.5:180, total RCS"}}
 
 
 def bodies_study(args, local: int) -> dict:
@@ -510,8 +593,10 @@ def batched_apply_study(args, local: int, wl: dict) -> dict:
     """The batched complex64 apply of 16 right-hand sides on the workload's
     sphere (mixed-precision plan): per-batch CUDA-event time with the leaf
     aggregation and far-field testing on the tensor cores (batch_tc.variant
-    1) and on the CUDA cores (0), against 16 single complex64 applies, and
-    the tensor-core rows' relative difference from the FP64 operator."""
+    1) and on the CUDA cores (0), with the tree passes once per level for all
+    slots (batch_tree.variant 1) and one slot after another (0), against 16
+    single complex64 applies, and the rows' relative difference from the FP64
+    operator."""
     import torch
     from mlfma_pmchwt_b200 import MLFMM
     from mlfma_pmchwt_b200 import mesh as M
@@ -541,6 +626,10 @@ def batched_apply_study(args, local: int, wl: dict) -> dict:
         out["ms_per_batch"]["tensor_cores" if v else "cuda_cores"] = round(
             timed(lambda: op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp), 3), 3)
     op.set_tuning("batch_tc.variant", 1)
+    op.set_tuning("batch_tree.variant", 0)
+    out["ms_per_batch"]["tensor_cores_tree_slot_by_slot"] = round(
+        timed(lambda: op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp), 3), 3)
+    op.set_tuning("batch_tree.variant", 1)
     out["ms_per_batch"]["16_single_applies"] = round(16 * timed(
         lambda: op.apply_mixed_device(X[0].data_ptr(), W[0].data_ptr(), sp), 10), 3)
     op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp)
@@ -763,6 +852,9 @@ def run_product(args):
         base = cpu_baseline_reference(args, wl, rank)
         if base:
             line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            solve_base = cpu_solve_baseline(args, local)
+            if solve_base:
+                line["cpu_baseline"]["solve"] = solve_base
     if rank == 0:
         print(json.dumps(line))
     op.close()
@@ -791,6 +883,8 @@ def main(argv=None):
     ap.add_argument("--plain-its", type=int, default=300, help="iteration cap of the plain GMRES comparison")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference matvecs to time")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-solve-its", type=int, default=300,
+                    help="iteration cap of the reference's GMRES(30) solve in the CPU baseline (0: skip)")
     ap.add_argument("--rhs", type=int, default=128, help="incidences of the multi-RHS study (0: skip)")
     ap.add_argument("--bodies", action="store_true", help="also run the 24-body uneven batch study")
     ap.add_argument("--no-mixed", dest="mixed", action="store_false",

@@ -111,6 +111,10 @@ SIGNATURES = {
     "mlfma_rhs_pmchwt": (C.c_int, [_P, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt": (C.c_int, [_P, _DP, C.c_int, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_pmchwt_noalloc": (C.c_int, [_P, _P, C.c_int, _DP, _DP, _P, _P]),
+    "mlfma_rhs_pmchwt_batch_device": (C.c_int, [_P, C.c_int, C.c_int, _DP, _DP, _DP, _P, _P]),
+    "mlfma_rcs_pmchwt_batch_device": (C.c_int, [_P, C.c_int, C.c_int, _P, C.c_int, _DP, _DP, _P, _P]),
+    "mlfma_rcs_pmchwt_mono_device": (C.c_int, [_P, C.c_int, C.c_int, _P, _DP, _DP, _P, _P]),
+    "mlfma_rcs_db": (C.c_int, [C.c_int, _DP, _DP, _DP, _DP]),
     "mlfma_rcs_noalloc_max_angles": (C.c_int, []),
     "mlfma_get_rwgs": (C.c_int, [_P, _IP, _IP, _IP, _IP, _IP, _IP, _DP, _DP]),
     "mlfma_get_level": (C.c_longlong, [_P, C.c_int, C.POINTER(C.c_ulonglong), _DP]),
@@ -156,6 +160,22 @@ def _ip(a: np.ndarray):
 
 def _c128(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def rcs_db(theta_deg, phi_deg, field) -> np.ndarray:
+    """RCS in dBsm (total, theta-pol, phi-pol) of far fields [n_angles, 3]
+    (complex), formed as the reference does (mlfma_rcs_db)."""
+    lib = load_library()
+    f = np.ascontiguousarray(field, dtype=np.complex128).reshape(-1, 3)
+    th = np.ascontiguousarray(np.atleast_1d(theta_deg), dtype=np.float64)
+    ph = np.ascontiguousarray(np.broadcast_to(np.atleast_1d(phi_deg), th.shape), dtype=np.float64)
+    if len(th) != len(f):
+        raise ValueError("one angle per field")
+    out = np.empty((len(th), 3))
+    rc = lib.mlfma_rcs_db(len(th), _dp(th), _dp(ph), _dp(f.view(np.float64)), _dp(out))
+    if rc < 0:
+        raise MlfmaError(rc, lib.mlfma_last_error().decode(errors="replace"))
+    return out
 
 
 def plane_wave(pol_deg: float, theta_deg: float, phi_deg: float):
@@ -343,7 +363,7 @@ class MLFMM:
     def get_tuning(self, key: str) -> int:
         return self._check(self._lib.mlfma_get_tuning(self._h, key.encode()))
 
-    TUNING_KEYS = (("m2l.variant", 9), ("up.variant", 4), ("l2l.variant", 2), ("agg.variant", 2), ("leaf.variant", 2), ("batch_tc.variant", 2), ("apply.graph", 2))
+    TUNING_KEYS = (("m2l.variant", 9), ("up.variant", 4), ("l2l.variant", 2), ("agg.variant", 2), ("leaf.variant", 2), ("batch_tc.variant", 2), ("batch_tree.variant", 2), ("near_batch.variant", 2), ("apply.graph", 2))
 
     def autotune(self, applies: int = 3) -> dict:
         """Times the values of each tuning key on this plan (one key at a
@@ -528,6 +548,37 @@ class MLFMM:
                                                _dp(field.view(np.float64)), _dp(db)))
         return field, db
 
+    def compute_v_pmchwt_batch_device(self, incidences, V_ptr: int, stream: int | None = None):
+        """Excitation vectors of R plane waves, incidences = [(kinc, einc, hinc), ...]
+        (as plane_wave returns them), into device complex128 [R, 2N] at V_ptr.
+        Asynchronous on `stream`."""
+        R = len(incidences)
+        k, e, h = (np.ascontiguousarray(np.array([inc[i] for inc in incidences], dtype=np.float64).reshape(R, 3))
+                   for i in range(3))
+        self._check(self._lib.mlfma_rhs_pmchwt_batch_device(self._h, self.n, R, _dp(k), _dp(e), _dp(h),
+                                                            C.c_void_p(V_ptr), C.c_void_p(stream or 0)))
+
+    def calculate_rcs_batch_device(self, R: int, I_ptr: int, theta_deg, phi_deg, field_ptr: int,
+                                   stream: int | None = None):
+        """Bistatic far field of R device current vectors (complex128 [R, 2N])
+        at the given angles into device complex128 [R, n_angles, 3]."""
+        th = np.ascontiguousarray(np.atleast_1d(theta_deg), dtype=np.float64)
+        ph = np.ascontiguousarray(np.broadcast_to(np.atleast_1d(phi_deg), th.shape), dtype=np.float64)
+        self._check(self._lib.mlfma_rcs_pmchwt_batch_device(self._h, self.n, int(R), C.c_void_p(I_ptr), len(th),
+                                                            _dp(th), _dp(ph), C.c_void_p(field_ptr),
+                                                            C.c_void_p(stream or 0)))
+
+    def calculate_rcs_mono_device(self, R: int, I_ptr: int, theta_deg, phi_deg, field_ptr: int,
+                                  stream: int | None = None):
+        """Monostatic far field: solution r seen at (theta_deg[r], phi_deg[r]),
+        into device complex128 [R, 3]."""
+        th = np.ascontiguousarray(np.atleast_1d(theta_deg), dtype=np.float64)
+        ph = np.ascontiguousarray(np.broadcast_to(np.atleast_1d(phi_deg), th.shape), dtype=np.float64)
+        if len(th) != R:
+            raise ValueError("one angle per solution")
+        self._check(self._lib.mlfma_rcs_pmchwt_mono_device(self._h, self.n, int(R), C.c_void_p(I_ptr), _dp(th),
+                                                           _dp(ph), C.c_void_p(field_ptr), C.c_void_p(stream or 0)))
+
     def calculate_rcs_noalloc(self, I_ptr: int, theta_deg, phi_deg, field_ptr: int, stream: int | None = None):
         """Far field into caller-owned device memory with no device allocation
         (see mlfma_rcs_pmchwt_noalloc): I_ptr -> complex128 [2N] on the device,
@@ -639,5 +690,5 @@ class MLFMM:
         return dict(target=t, source=s, z12=z)
 
 
-__all__ = ["MLFMM", "Mesh", "MlfmaError", "load_library", "plane_wave", "mesh_mod", "SIGNATURES", "LIB_PATH",
+__all__ = ["MLFMM", "Mesh", "MlfmaError", "load_library", "plane_wave", "rcs_db", "mesh_mod", "SIGNATURES", "LIB_PATH",
            "lp_param_count", "lp_adam_device"]

@@ -139,6 +139,7 @@ struct UpArg {
   const double* lp;
   const C* ph_up;
   int Kp, nphp, Kc, nphc;
+  long long slot_c = 0, slot_p = 0;  // element strides between right-hand-side slots (grid.z = 6 x slots)
 };
 
 // One thread per (parent box, parent direction, component): the 9-tap
@@ -150,7 +151,8 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
   using R = typename Cx<C>::real;
   const int kk = blockIdx.y * blockDim.x + threadIdx.x;
   const int b = blockIdx.x;
-  const int c = blockIdx.z;
+  const int slot = blockIdx.z / 6;
+  const int c = blockIdx.z - 6 * slot;
   if (kk >= a.Kp) return;
   const int t = kk / a.nphp, p = kk - t * a.nphp;
   int ti[3], pi[3];
@@ -166,7 +168,7 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
   const int c1 = a.child_begin[b + 1];
   for (int ch = a.child_begin[b]; ch < c1; ++ch) {
     const C e = __ldg(a.ph_up + a.octant[ch] * a.Kp + kk);
-    const C* sc = a.Sc + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
+    const C* sc = a.Sc + slot * a.slot_c + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
     C v = Cx<C>::zero();
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -174,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
       for (int j = 0; j < 3; ++j) v = cfmas(static_cast<R>(wt[i] * wp[j]), __ldg(sc + ti[i] + pi[j]), v);
     acc = cfma(e, v, acc);
   }
-  a.Sp[(static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
+  a.Sp[slot * a.slot_p + (static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
 }
 
 // Interpolation (m2m), one thread per (parent box, parent direction) for all
@@ -713,6 +715,7 @@ struct M2lPairSeg {
   const int* pair_src;
   const int2* pair_vec;
   int B, K, nchunk, cta_begin;
+  long long slot_S = 0, slot_B = 0;  // element strides between right-hand-side slots (grid.y = slots)
 };
 template <class C>
 struct M2lPairArg {
@@ -731,6 +734,8 @@ __global__ void __launch_bounds__(32 * kPairWarps) m2l_pair_kernel(const __grid_
   const int k = (local - grp * g.nchunk) * 32 + (threadIdx.x & 31);
   const int K = g.K;
   if (2 * pg >= g.B || k >= K) return;
+  const C* const Sl = g.S + blockIdx.y * g.slot_S;
+  C* const Bl = g.Bm + blockIdx.y * g.slot_B;
   C a0[6], a1[6];
 #pragma unroll
   for (int c = 0; c < 6; ++c) a0[c] = a1[c] = Cx<C>::zero();
@@ -738,7 +743,7 @@ __global__ void __launch_bounds__(32 * kPairWarps) m2l_pair_kernel(const __grid_
   for (int e = g.pair_ptr[pg]; e < e1; ++e) {
     const int src = __ldg(g.pair_src + e);
     const int2 v = __ldg(g.pair_vec + e);
-    const C* p = g.S + static_cast<size_t>(src) * 6 * K + k;
+    const C* p = Sl + static_cast<size_t>(src) * 6 * K + k;
     C sv[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) sv[c] = __ldg(p + static_cast<size_t>(c) * K);
@@ -753,11 +758,11 @@ __global__ void __launch_bounds__(32 * kPairWarps) m2l_pair_kernel(const __grid_
       for (int c = 0; c < 6; ++c) a1[c] = cfma(t, sv[c], a1[c]);
     }
   }
-  C* out0 = g.Bm + static_cast<size_t>(2 * pg) * 6 * K + k;
+  C* out0 = Bl + static_cast<size_t>(2 * pg) * 6 * K + k;
 #pragma unroll
   for (int c = 0; c < 6; ++c) out0[static_cast<size_t>(c) * K] = a0[c];
   if (2 * pg + 1 < g.B) {
-    C* out1 = g.Bm + static_cast<size_t>(2 * pg + 1) * 6 * K + k;
+    C* out1 = Bl + static_cast<size_t>(2 * pg + 1) * 6 * K + k;
 #pragma unroll
     for (int c = 0; c < 6; ++c) out1[static_cast<size_t>(c) * K] = a1[c];
   }
@@ -1076,6 +1081,7 @@ struct L2lSepArg {
   const int* ph_src;
   const double* ph_w;
   int ntc, npc, ntp, npp;
+  long long slot_c = 0, slot_p = 0;  // element strides between right-hand-side slots (grid.z = slots)
 };
 
 constexpr int kL2lBand = 2944;     // band entries in shared memory (46 KiB), all 6 components
@@ -1109,8 +1115,8 @@ __global__ void __launch_bounds__(256, 4) l2l_sep_kernel(L2lSepArg<C> a) {
   const int band_rows = l2l_band_rows(a.ntc, a.npp);
   const int Kp = a.ntp * a.npp, Kc = a.ntc * a.npc;
   const C* ph = a.ph_dn + a.octant[b] * Kp;
-  const C* bp = a.Bp + static_cast<size_t>(a.parent[b]) * 6 * Kp;
-  C* out = a.Bm + static_cast<size_t>(b) * 6 * Kc;
+  const C* bp = a.Bp + blockIdx.z * a.slot_p + static_cast<size_t>(a.parent[b]) * 6 * Kp;
+  C* out = a.Bm + blockIdx.z * a.slot_c + static_cast<size_t>(b) * 6 * Kc;
   for (int tc0 = blockIdx.y * band_rows; tc0 < a.ntc; tc0 += gridDim.y * band_rows) {
     const int rows = min(band_rows, a.ntc - tc0);
     const int stride = rows * a.npp;
@@ -1694,6 +1700,58 @@ void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s, cudaStr
   }
 }
 
+// The tree passes of medium m for rn right-hand-side slots at once (mixed
+// plans): every level's interpolation, translation and anterpolation is one
+// launch over all slots of the slot-major arrays btS / btB (the slot is a grid
+// dimension), with the kernels of tree_pass_fixed. The leaf level's
+// translation runs on sx beside the interpolation chain, as there.
+void tree_pass_slots(Plan& P, int m, int rn, cudaStream_t s, cudaStream_t sx, cudaEvent_t ev_agg,
+                     cudaEvent_t ev_leaf) {
+  using C = float2;
+  const int L = P.maxL;
+  auto stride = [&](int l) { return static_cast<long long>(P.lv[l].B) * 6 * P.ml[m][l].K; };
+  auto translate = [&](int lo, int hi, cudaStream_t st) {
+    if (lo > hi) return;
+    if (hi - lo + 1 > kM2lMaxSeg) throw std::runtime_error("m2l: more levels than one launch takes");
+    M2lPairArg<C> t{};
+    int ctas = 0;
+    for (int l = lo; l <= hi; ++l) {
+      const MediumLevel& cm = P.ml[m][l];
+      M2lPairSeg<C>& g = t.seg[t.nseg++];
+      g = M2lPairSeg<C>{P.btS[m][l],      P.btB[m][l], cm.tfw32,          P.lv[l].pair_ptr, P.lv[l].pair_src,
+                        P.lv[l].pair_vec, P.lv[l].B,   cm.K,              (cm.K + 31) / 32, ctas,
+                        stride(l),        stride(l)};
+      ctas += (((P.lv[l].B + 1) / 2 + kPairWarps - 1) / kPairWarps) * g.nchunk;
+    }
+    m2l_pair_kernel<C><<<dim3(ctas, rn), 32 * kPairWarps, 0, st>>>(t);
+    MLFMA_CUDA(cudaGetLastError());
+  };
+  MLFMA_CUDA(cudaEventRecord(ev_agg, s));
+  MLFMA_CUDA(cudaStreamWaitEvent(sx, ev_agg, 0));
+  translate(L, L, sx);
+  MLFMA_CUDA(cudaEventRecord(ev_leaf, sx));
+  for (int l = L - 1; l >= 2; --l) {
+    const MediumLevel& pm = P.ml[m][l];
+    const MediumLevel& cm = P.ml[m][l + 1];
+    UpArg<C> a{P.btS[m][l + 1], P.btS[m][l], P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx,
+               pm.lp,           pm.ph_up32,  pm.K,                 pm.nph,              cm.K,    cm.nph,
+               stride(l + 1),   stride(l)};
+    up_kernel<C><<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6 * rn), kThreads, 0, s>>>(a);
+  }
+  translate(2, L - 1, s);
+  MLFMA_CUDA(cudaStreamWaitEvent(s, ev_leaf, 0));
+  for (int l = 3; l <= L; ++l) {
+    const MediumLevel& cm = P.ml[m][l];
+    const MediumLevel& pm = P.ml[m][l - 1];
+    if (6 * pm.nph > kL2lBand) throw std::runtime_error("anterpolation band: phi grid too large for this precision");
+    L2lSepArg<C> b{P.btB[m][l], P.btB[m][l - 1], P.lv[l].parent, P.lv[l].octant, pm.ph_dn32, cm.thT_ptr,
+                   cm.thT_src,  cm.thT_w,        cm.phT_ptr,     cm.phT_src,     cm.phT_w,   cm.nth,
+                   cm.nph,      pm.nth,          pm.nph,         stride(l),      stride(l - 1)};
+    l2l_sep_kernel<C><<<dim3(P.lv[l].B, l2l_grid_y(P.lv[l].B, cm.nth, pm.nph), rn), 256, 0, s>>>(b);
+  }
+  MLFMA_CUDA(cudaGetLastError());
+}
+
 template <class C>
 void apply_fixed(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   const int L = P.maxL;
@@ -1770,8 +1828,20 @@ void apply_batch_fixed(Plan& P, int R, const double2* X, long long ldx, double2*
       agg_batch_kernel<C, kAggRB><<<dim3(P.lv[L].B, 2, (rn + kAggRB - 1) / kAggRB), kThreads, 0, s>>>(ag);
     {
       MediumStreams ms(P, s, true);
-      for (int j = 0; j < rn; ++j)
-        for (int m = 0; m < 2; ++m) tree_pass_fixed<C>(P, m, Store<C>::bS(P, m, j), Store<C>::bB(P, m, j), ms.of(m));
+      if constexpr (std::is_same<C, float2>::value) {
+        if (P.tuning.batch_tree == 1) {
+          for (int m = 0; m < 2; ++m)
+            tree_pass_slots(P, m, rn, ms.of(m), P.stream_leaf[m], P.ev_agg[m], P.ev_leaf[m]);
+        } else {
+          for (int j = 0; j < rn; ++j)
+            for (int m = 0; m < 2; ++m)
+              tree_pass_fixed<C>(P, m, Store<C>::bS(P, m, j), Store<C>::bB(P, m, j), ms.of(m));
+        }
+      } else {
+        for (int j = 0; j < rn; ++j)
+          for (int m = 0; m < 2; ++m)
+            tree_pass_fixed<C>(P, m, Store<C>::bS(P, m, j), Store<C>::bB(P, m, j), ms.of(m));
+      }
       ms.join();
     }
     LeafBatchArg<C> lb{};
@@ -1898,15 +1968,26 @@ void apply_direct(Plan& P, const double2* x, double2* w, cudaStream_t s) {
 void reserve_batch(Plan& P, int R) {
   const int want = std::min(R, kBatchSlots);
   const int L = P.maxL;
+  if (P.precision == 1 && P.bS32[0].empty()) {
+    // the complex64 tree of every slot at once, slot-major per level
+    for (int m = 0; m < 2; ++m) {
+      for (int l = 2; l <= L; ++l) {
+        const size_t cnt = static_cast<size_t>(P.lv[l].B) * 6 * P.ml[m][l].K;
+        P.btS[m][l] = P.alloc<float2>(kBatchSlots * cnt);
+        P.btB[m][l] = P.alloc<float2>(kBatchSlots * cnt);
+      }
+      const size_t cnt = static_cast<size_t>(P.lv[L].B) * 6 * P.ml[m][L].K;
+      for (int j = 0; j < kBatchSlots; ++j) {
+        P.bS32[m].push_back(P.btS[m][L] + j * cnt);
+        P.bB32[m].push_back(P.btB[m][L] + j * cnt);
+      }
+    }
+  }
   while (P.batch_cap < want) {
     for (int m = 0; m < 2; ++m) {
       const size_t cnt = static_cast<size_t>(P.lv[L].B) * 6 * P.ml[m][L].K;
       P.bS[m].push_back(P.alloc<double2>(cnt));
       P.bB[m].push_back(P.alloc<double2>(cnt));
-      if (P.precision == 1) {
-        P.bS32[m].push_back(P.alloc<float2>(cnt));
-        P.bB32[m].push_back(P.alloc<float2>(cnt));
-      }
     }
     ++P.batch_cap;
   }

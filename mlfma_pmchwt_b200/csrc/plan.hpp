@@ -130,6 +130,10 @@ struct Tuning {
                                //    the box's contiguous pattern block
   int batch_tc = 1;            // batched complex64 leaf aggregation and far-field testing: 0 CUDA cores; 1 tcgen05
                                //    (3xTF32 split, TMEM accumulators)
+  int batch_tree = 1;          // batched complex64 tree passes: 0 one slot after another; 1 every level
+                               //    once for all slots (slot-major arrays)
+  int near_batch = 1;          // lockstep preconditioner's near-field product: 0 lanes over sources;
+                               //    1 lanes over systems (groups of 8 or more)
   int leaf_variant = 0;        // 0: near field inside the leaf kernel; 1: near field on its own
                                //    stream from the start of the apply, the leaf kernel adds the far field
   int graph = 1;               // 1: capture each apply (per x, w, stream and precision) as a CUDA
@@ -220,6 +224,12 @@ struct Plan {
   int batch_cap = 0;
   std::vector<double2*> bS[2], bB[2];
   std::vector<float2*> bS32[2], bB32[2];
+  // Complex64 tree arrays of all kBatchSlots right-hand-side slots (mixed
+  // plans), per medium and level 2..maxLevel, slot-major and contiguous:
+  // [slot][B][6][K]. bS32 / bB32 point into the leaf level's arrays. The
+  // batched complex64 apply runs every tree pass once per level for all slots.
+  float2* btS[2][16] = {};
+  float2* btB[2][16] = {};
   double2* d_xb = nullptr;          // staging for host-pointer batched apply
   double2* d_wb = nullptr;
   int xb_cap = 0;
