@@ -626,10 +626,12 @@ def batched_apply_study(args, local: int, wl: dict) -> dict:
         out["ms_per_batch"]["tensor_cores" if v else "cuda_cores"] = round(
             timed(lambda: op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp), 3), 3)
     op.set_tuning("batch_tc.variant", 1)
-    op.set_tuning("batch_tree.variant", 0)
-    out["ms_per_batch"]["tensor_cores_tree_slot_by_slot"] = round(
-        timed(lambda: op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp), 3), 3)
-    op.set_tuning("batch_tree.variant", 1)
+    tree_keep = op.get_tuning("batch_tree.variant")
+    for v, key in ((0, "tensor_cores_tree_slot_by_slot"), (1, "tensor_cores_tree_slot_grid")):
+        op.set_tuning("batch_tree.variant", v)
+        out["ms_per_batch"][key] = round(
+            timed(lambda: op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp), 3), 3)
+    op.set_tuning("batch_tree.variant", tree_keep)
     out["ms_per_batch"]["16_single_applies"] = round(16 * timed(
         lambda: op.apply_mixed_device(X[0].data_ptr(), W[0].data_ptr(), sp), 10), 3)
     op.apply_batch_mixed_device(R, X.data_ptr(), W.data_ptr(), sp)
@@ -840,7 +842,7 @@ def run_product(args):
         line["batched_apply"] = batched_apply_study(args, local, wl)
     if args.rhs > 0 and world == 1:
         line["multi_rhs"] = multi_rhs_study(args, local)
-    if args.bodies and world == 1:
+    if args.bodies and args.size == "full" and world == 1:
         line["uneven_bodies"] = bodies_study(args, local)
     if args.full_rhs and args.size == "full" and world == 1:
         line["multi_rhs_full"] = full_rhs_study(args, local)
@@ -886,7 +888,8 @@ def main(argv=None):
     ap.add_argument("--cpu-solve-its", type=int, default=300,
                     help="iteration cap of the reference's GMRES(30) solve in the CPU baseline (0: skip)")
     ap.add_argument("--rhs", type=int, default=128, help="incidences of the multi-RHS study (0: skip)")
-    ap.add_argument("--bodies", action="store_true", help="also run the 24-body uneven batch study")
+    ap.add_argument("--no-bodies", dest="bodies", action="store_false",
+                    help="skip the 24-body uneven batch study (run by default on the full-size workload)")
     ap.add_argument("--no-mixed", dest="mixed", action="store_false",
                     help="skip the complex64 (mixed-precision) operator and solve")
     ap.add_argument("--batched-only", action="store_true",
@@ -900,7 +903,7 @@ def main(argv=None):
                     help="training ellipsoids of the learned-preconditioner study")
     ap.add_argument("--learned-epochs", type=int, default=10)
     ap.add_argument("--bodies-workers", type=int, default=4,
-                    help="bodies solved at once by the --bodies study (host threads, one plan each)")
+                    help="bodies solved at once by the uneven-body study (host threads, one plan each)")
     ap.add_argument("--tuning", default="auto",
                     help="'auto' (autotune) or fixed kernel variants, e.g. m2l.variant=2,up.variant=1")
     args = ap.parse_args(argv)

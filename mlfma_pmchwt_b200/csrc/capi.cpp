@@ -299,7 +299,6 @@ constexpr TuningKey kTuningKeys[] = {
     {"leaf.variant", &mlfma::Tuning::leaf_variant, 2},
     {"batch_tc.variant", &mlfma::Tuning::batch_tc, 2},
     {"batch_tree.variant", &mlfma::Tuning::batch_tree, 2},
-    {"near_batch.variant", &mlfma::Tuning::near_batch, 2},
     {"apply.graph", &mlfma::Tuning::graph, 2},
 };
 const TuningKey* find_key(const char* key) {
@@ -353,8 +352,7 @@ int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms) {
     // one key at a time, the others held at their current (best so far) value
     int slot = 0;
     for (const TuningKey& k : kTuningKeys) {
-      if (k.field == &mlfma::Tuning::batch_tc || k.field == &mlfma::Tuning::batch_tree ||
-          k.field == &mlfma::Tuning::near_batch) {  // no effect on the single apply timed here
+      if (k.field == &mlfma::Tuning::batch_tc || k.field == &mlfma::Tuning::batch_tree) {  // no effect on the single apply timed here
         if (variant_ms)
           for (int v = 0; v < k.count; ++v) variant_ms[slot + v] = -1.0;
         slot += k.count;

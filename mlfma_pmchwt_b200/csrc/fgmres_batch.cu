@@ -309,58 +309,6 @@ __global__ void __launch_bounds__(128) near_batch_box_kernel(NearBatchArg<Z> a) 
   }
 }
 
-// The same products with the systems across the lanes: one CTA per (leaf box,
-// group of kNearSysRB systems), the box's source values of the group staged
-// once in shared memory as [source][system] (J and M of a system in one
-// 16-byte word), and each half-warp forms one target row for the group's 16
-// systems (lane = system), walking the row's sources in order. Every near-field
-// entry is then read once per 16 systems, with one broadcast load per half-warp,
-// and no cross-lane reduction is needed. The sums run over the sources in
-// order, so they differ from near_batch_kernel's only by rounding.
-constexpr int kNearSysRB = 16;
-
-__global__ void __launch_bounds__(256, 2) near_batch_sys_kernel(NearBatchArg<float2> a) {
-  extern __shared__ __align__(16) unsigned char near_smem[];
-  float4* xsm = reinterpret_cast<float4*>(near_smem);  // [source][system]: J (x, y), M (z, w)
-  const int b = blockIdx.x;
-  const int p0 = blockIdx.y * kNearSysRB, pn = min(kNearSysRB, a.R - p0);
-  const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
-  const int r0 = a.leaf_ptr[b], nb = a.leaf_ptr[b + 1] - r0;
-  for (int i = threadIdx.x; i < kNearSysRB * ns; i += blockDim.x) {
-    const int j = i / ns, q = i - j * ns;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (j < pn) {
-      const double2* xj = a.x.at(p0 + j, a.sys);
-      const int src = a.near_src[s0 + q];
-      const double2 J = xj[src], M = xj[a.N + src];
-      v = make_float4(static_cast<float>(J.x), static_cast<float>(J.y), static_cast<float>(M.x),
-                      static_cast<float>(M.y));
-    }
-    xsm[q * kNearSysRB + j] = v;
-  }
-  __syncthreads();
-  const int j = threadIdx.x & (kNearSysRB - 1);
-  const int nhw = blockDim.x / kNearSysRB;
-  for (int tl = threadIdx.x / kNearSysRB; tl < nb; tl += nhw) {
-    const float2* Zr = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
-    float2 nJ = make_float2(0.f, 0.f), nM = make_float2(0.f, 0.f);
-#pragma unroll 4
-    for (int q = 0; q < ns; ++q) {
-      const float2 z11 = Zr[3 * q], z12 = Zr[3 * q + 1], z22 = Zr[3 * q + 2];
-      const float4 x = xsm[q * kNearSysRB + j];
-      const float2 xJ = make_float2(x.x, x.y), xM = make_float2(x.z, x.w);
-      nJ = cfma(z11, xJ, cfma(z12, xM, nJ));
-      nM = cfma(z22, xM, csub(nM, cmul(z12, xJ)));
-    }
-    if (j < pn) {
-      const int id = a.leaf_rwg[r0 + tl];
-      double2* w = a.w.at(p0 + j, a.sys);
-      w[id] = Cx<float2>::to64(nJ);
-      w[a.N + id] = Cx<float2>::to64(nM);
-    }
-  }
-}
-
 // Upper-triangular solve of the rotated least-squares system (Code/GMRES.h:165-182).
 void back_substitute(const std::vector<C>& H, int ld, const std::vector<C>& s, int m, std::vector<C>& y) {
   const double eps = 1e-16;
@@ -530,11 +478,6 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   if (inner_its > 0 && box_smem <= kNearBoxSmemMax)
     MLFMA_CUDA(cudaFuncSetAttribute(near_batch_box_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(box_smem)));
-  const size_t sys_smem = static_cast<size_t>(kNearSysRB) * ns_max * sizeof(float4);
-  const bool sys_ok = P.tuning.near_batch == 1 && sys_smem <= kNearBoxSmemMax;
-  if (inner_its > 0 && sys_ok)
-    MLFMA_CUDA(cudaFuncSetAttribute(near_batch_sys_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(sys_smem)));
   // z_q = (inner_its GMRES steps on Z_near from zero) applied to v_q, q in list
   auto precondition = [&](const std::vector<int>& list, long long voff, long long zoff) {
     const int Ra = static_cast<int>(list.size());
@@ -557,10 +500,7 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
                                 P.d_near_sptr, P.d_near_src,         P.d_near_zoff,
                                 P.d_near_z32,  sysref(Q, qs, j * n), sysref(Q, qs, (j + 1) * n),
                                 sysd,          P.N,                  Ra};
-        if (sys_ok && Ra >= kNearSysRB / 2) {
-          const dim3 ng(nleaf, (Ra + kNearSysRB - 1) / kNearSysRB);
-          near_batch_sys_kernel<<<ng, 256, sys_smem, s>>>(na);
-        } else if (box_smem <= kNearBoxSmemMax) {
+        if (box_smem <= kNearBoxSmemMax) {
           const dim3 ng(nleaf, (Ra + kNearBoxRB - 1) / kNearBoxRB);
           near_batch_box_kernel<float2><<<ng, 128, box_smem, s>>>(na);
         } else {

@@ -132,8 +132,6 @@ struct Tuning {
                                //    (3xTF32 split, TMEM accumulators)
   int batch_tree = 1;          // batched complex64 tree passes: 0 one slot after another; 1 every level
                                //    once for all slots (slot-major arrays)
-  int near_batch = 1;          // lockstep preconditioner's near-field product: 0 lanes over sources;
-                               //    1 lanes over systems (groups of 8 or more)
   int leaf_variant = 0;        // 0: near field inside the leaf kernel; 1: near field on its own
                                //    stream from the start of the apply, the leaf kernel adds the far field
   int graph = 1;               // 1: capture each apply (per x, w, stream and precision) as a CUDA

@@ -133,8 +133,8 @@ def test_tensor_core_batched_apply_large_leaf_boxes(leaf, tc_path):
 def test_slot_batched_tree_passes(case_files, name, R):
     """The batched complex64 apply with every tree pass launched once per
     level for all slots (batch_tree.variant 1, slot-major arrays) against the
-    same apply one slot after another (0): the same kernels per slot, so the
-    rows agree to complex64 rounding of identical arithmetic."""
+    same apply one slot after another (0): the same arithmetic per slot, so
+    the rows agree to complex64 rounding of identical operations."""
     import torch
     from mlfma_pmchwt_b200 import mesh as M
     op = mixed_op(case_files, name)
@@ -154,24 +154,3 @@ def test_slot_batched_tree_passes(case_files, name, R):
         assert rel(outs[1][j], outs[0][j]) < 1e-12, j
         assert rel(outs[1][j], ref[j]) < 1e-5, j
 
-
-def test_near_product_variants_in_the_lockstep_solve(case_files):
-    """The lockstep solve's near-field products with the systems across the
-    lanes (near_batch.variant 1, taken for groups of 8 or more) against the
-    sources across the lanes (0): same preconditioner up to complex64
-    rounding, so both solves converge in about the same iterations to the
-    same solutions."""
-    from mlfma_pmchwt_b200 import plane_wave
-    op = mixed_op(case_files, "sphere_s3_lossy")
-    R = 12
-    B = np.stack([op.compute_v_pmchwt(*plane_wave(90.0 * (j % 2), 180.0 * j / (R - 1), 0.0)) for j in range(R)])
-    out = {}
-    for v in (0, 1):
-        op.set_tuning("near_batch.variant", v)
-        X, st = op.matrix_solver_batch(B, itr_max=2000, mr=50, tol_abs=0.0, tol_rel=1e-8, inner_its=8)
-        assert all(s["converged"] for s in st), v
-        out[v] = (X, [s["iterations"] for s in st])
-    op.set_tuning("near_batch.variant", 1)
-    for j in range(R):
-        assert rel(out[1][0][j], out[0][0][j]) < 1e-6, j
-        assert abs(out[1][1][j] - out[0][1][j]) <= 2, j

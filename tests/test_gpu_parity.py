@@ -306,7 +306,7 @@ def test_kernel_variants_agree(case_files, ref_ops, name):
     res = op.autotune(2)
     for key, cnt in op.TUNING_KEYS:
         assert 0 <= res[key] < cnt and len(res[key + "_ms"]) == cnt
-        if key in ("batch_tc.variant", "batch_tree.variant", "near_batch.variant"):  # batched paths only: not timed
+        if key in ("batch_tc.variant", "batch_tree.variant"):  # batched paths only: not timed
             assert all(v == -1.0 for v in res[key + "_ms"])
         else:
             assert min(res[key + "_ms"]) > 0
