@@ -466,8 +466,10 @@ void launch_agg_tc(const Plan& P, const AggTcArg& a, cudaStream_t s) {
   if (a.kmax % 8 != 0 || a.kmax < 8 || a.kmax > kAggTcMaxRwgs)
     throw std::invalid_argument("tensor-core aggregation: leaf boxes hold too many RWGs");
   const size_t smem = agg_tc_smem_bytes(a.kmax);
-  MLFMA_CUDA(
-      cudaFuncSetAttribute(agg_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  // the limit is the largest any plan uses, the same value on every call: plans
+  // launched from several host threads then never lower it under another's launch
+  MLFMA_CUDA(cudaFuncSetAttribute(agg_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(agg_tc_smem_bytes(kAggTcMaxRwgs))));
   agg_tc_kernel<<<dim3(P.lv[P.maxL].B, 2), 128, smem, s>>>(a);
   MLFMA_CUDA(cudaGetLastError());
 }

@@ -475,9 +475,12 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   int ns_max = 0;
   for (int bx = 0; bx < nleaf; ++bx) ns_max = std::max(ns_max, P.h_near_sptr[bx + 1] - P.h_near_sptr[bx]);
   const size_t box_smem = static_cast<size_t>(2 * kNearBoxRB) * ns_max * sizeof(float2);
+  // The shared-memory limit is set to the same largest value on every call:
+  // solves of several plans from several host threads then never lower it
+  // under another's launch.
   if (inner_its > 0 && box_smem <= kNearBoxSmemMax)
     MLFMA_CUDA(cudaFuncSetAttribute(near_batch_box_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(box_smem)));
+                                    static_cast<int>(kNearBoxSmemMax)));
   // z_q = (inner_its GMRES steps on Z_near from zero) applied to v_q, q in list
   auto precondition = [&](const std::vector<int>& list, long long voff, long long zoff) {
     const int Ra = static_cast<int>(list.size());

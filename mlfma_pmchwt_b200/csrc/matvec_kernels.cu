@@ -146,12 +146,14 @@ struct UpArg {
 // separable interpolation of each child's pattern, times the child's shift
 // phase, summed over the children. One component per thread keeps the
 // register count low enough for the occupancy this gather needs.
-template <class C>
+// kSlots: grid.z = 6 x slots with the slot offsets of the batched tree; the
+// single apply instantiates without them.
+template <class C, bool kSlots = false>
 __global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
   using R = typename Cx<C>::real;
   const int kk = blockIdx.y * blockDim.x + threadIdx.x;
   const int b = blockIdx.x;
-  const int slot = blockIdx.z / 6;
+  const int slot = kSlots ? blockIdx.z / 6 : 0;
   const int c = blockIdx.z - 6 * slot;
   if (kk >= a.Kp) return;
   const int t = kk / a.nphp, p = kk - t * a.nphp;
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
   const int c1 = a.child_begin[b + 1];
   for (int ch = a.child_begin[b]; ch < c1; ++ch) {
     const C e = __ldg(a.ph_up + a.octant[ch] * a.Kp + kk);
-    const C* sc = a.Sc + slot * a.slot_c + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
+    const C* sc = (kSlots ? a.Sc + slot * a.slot_c : a.Sc) + (static_cast<size_t>(ch) * 6 + c) * a.Kc;
     C v = Cx<C>::zero();
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
       for (int j = 0; j < 3; ++j) v = cfmas(static_cast<R>(wt[i] * wp[j]), __ldg(sc + ti[i] + pi[j]), v);
     acc = cfma(e, v, acc);
   }
-  a.Sp[slot * a.slot_p + (static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
+  (kSlots ? a.Sp + slot * a.slot_p : a.Sp)[(static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
 }
 
 // Interpolation (m2m), one thread per (parent box, parent direction) for all
@@ -723,7 +725,10 @@ struct M2lPairArg {
   int nseg;
 };
 
-template <class C>
+// kSlots: the slot offsets of the batched tree (grid.y = slot); the single
+// apply instantiates without them (two registers fewer: 96 rather than 98 in
+// FP64, which keeps five CTAs per SM).
+template <class C, bool kSlots = false>
 __global__ void __launch_bounds__(32 * kPairWarps) m2l_pair_kernel(const __grid_constant__ M2lPairArg<C> a) {
   int si = 0;
   while (si + 1 < a.nseg && static_cast<int>(blockIdx.x) >= a.seg[si + 1].cta_begin) ++si;
@@ -734,8 +739,8 @@ __global__ void __launch_bounds__(32 * kPairWarps) m2l_pair_kernel(const __grid_
   const int k = (local - grp * g.nchunk) * 32 + (threadIdx.x & 31);
   const int K = g.K;
   if (2 * pg >= g.B || k >= K) return;
-  const C* const Sl = g.S + blockIdx.y * g.slot_S;
-  C* const Bl = g.Bm + blockIdx.y * g.slot_B;
+  const C* const Sl = kSlots ? g.S + blockIdx.y * g.slot_S : g.S;
+  C* const Bl = kSlots ? g.Bm + blockIdx.y * g.slot_B : g.Bm;
   C a0[6], a1[6];
 #pragma unroll
   for (int c = 0; c < 6; ++c) a0[c] = a1[c] = Cx<C>::zero();
@@ -1107,7 +1112,9 @@ inline int l2l_grid_y(int boxes, int ntc, int npp) {
 // reference's 9-tap weight of a (parent, child) direction pair is the
 // product of the two 1-D weights used here (Code/AlgoMLFMM.h:347-351).
 // (4 CTAs per SM: 64 registers, up from 3 CTAs at 80.)
-template <class C>
+// kSlots: grid.z = slots with the slot offsets of the batched tree; the single
+// apply instantiates without them.
+template <class C, bool kSlots = false>
 __global__ void __launch_bounds__(256, 4) l2l_sep_kernel(L2lSepArg<C> a) {
   using R = typename Cx<C>::real;
   __shared__ C band[kL2lBand];
@@ -1115,8 +1122,8 @@ __global__ void __launch_bounds__(256, 4) l2l_sep_kernel(L2lSepArg<C> a) {
   const int band_rows = l2l_band_rows(a.ntc, a.npp);
   const int Kp = a.ntp * a.npp, Kc = a.ntc * a.npc;
   const C* ph = a.ph_dn + a.octant[b] * Kp;
-  const C* bp = a.Bp + blockIdx.z * a.slot_p + static_cast<size_t>(a.parent[b]) * 6 * Kp;
-  C* out = a.Bm + blockIdx.z * a.slot_c + static_cast<size_t>(b) * 6 * Kc;
+  const C* bp = (kSlots ? a.Bp + blockIdx.z * a.slot_p : a.Bp) + static_cast<size_t>(a.parent[b]) * 6 * Kp;
+  C* out = (kSlots ? a.Bm + blockIdx.z * a.slot_c : a.Bm) + static_cast<size_t>(b) * 6 * Kc;
   for (int tc0 = blockIdx.y * band_rows; tc0 < a.ntc; tc0 += gridDim.y * band_rows) {
     const int rows = min(band_rows, a.ntc - tc0);
     const int stride = rows * a.npp;
@@ -1723,7 +1730,7 @@ void tree_pass_slots(Plan& P, int m, int rn, cudaStream_t s, cudaStream_t sx, cu
                         stride(l),        stride(l)};
       ctas += (((P.lv[l].B + 1) / 2 + kPairWarps - 1) / kPairWarps) * g.nchunk;
     }
-    m2l_pair_kernel<C><<<dim3(ctas, rn), 32 * kPairWarps, 0, st>>>(t);
+    m2l_pair_kernel<C, true><<<dim3(ctas, rn), 32 * kPairWarps, 0, st>>>(t);
     MLFMA_CUDA(cudaGetLastError());
   };
   MLFMA_CUDA(cudaEventRecord(ev_agg, s));
@@ -1736,7 +1743,7 @@ void tree_pass_slots(Plan& P, int m, int rn, cudaStream_t s, cudaStream_t sx, cu
     UpArg<C> a{P.btS[m][l + 1], P.btS[m][l], P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx,
                pm.lp,           pm.ph_up32,  pm.K,                 pm.nph,              cm.K,    cm.nph,
                stride(l + 1),   stride(l)};
-    up_kernel<C><<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6 * rn), kThreads, 0, s>>>(a);
+    up_kernel<C, true><<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6 * rn), kThreads, 0, s>>>(a);
   }
   translate(2, L - 1, s);
   MLFMA_CUDA(cudaStreamWaitEvent(s, ev_leaf, 0));
@@ -1747,7 +1754,7 @@ void tree_pass_slots(Plan& P, int m, int rn, cudaStream_t s, cudaStream_t sx, cu
     L2lSepArg<C> b{P.btB[m][l], P.btB[m][l - 1], P.lv[l].parent, P.lv[l].octant, pm.ph_dn32, cm.thT_ptr,
                    cm.thT_src,  cm.thT_w,        cm.phT_ptr,     cm.phT_src,     cm.phT_w,   cm.nth,
                    cm.nph,      pm.nth,          pm.nph,         stride(l),      stride(l - 1)};
-    l2l_sep_kernel<C><<<dim3(P.lv[l].B, l2l_grid_y(P.lv[l].B, cm.nth, pm.nph), rn), 256, 0, s>>>(b);
+    l2l_sep_kernel<C, true><<<dim3(P.lv[l].B, l2l_grid_y(P.lv[l].B, cm.nth, pm.nph), rn), 256, 0, s>>>(b);
   }
   MLFMA_CUDA(cudaGetLastError());
 }

@@ -154,3 +154,4 @@ def test_slot_batched_tree_passes(case_files, name, R):
         assert rel(outs[1][j], outs[0][j]) < 1e-12, j
         assert rel(outs[1][j], ref[j]) < 1e-5, j
 
+
