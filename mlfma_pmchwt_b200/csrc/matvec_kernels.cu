@@ -1474,7 +1474,7 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
 // Translations of levels lo..hi of medium m (independent of each other).
 void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s, int lo, int hi) {
   if (lo > hi) return;
-  if (P.tuning.m2l_variant >= 6) {
+  if (P.tuning.m2l_variant >= 6 && P.tuning.m2l_variant <= 8) {
     launch_m2l_grp<double2>(
         P, lo, hi, P.tuning.m2l_variant == 6 ? 2 : 4, P.tuning.m2l_variant == 8,
         [&](int l) { return level_S(P, m, l, v); },
@@ -1656,7 +1656,7 @@ void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s, cudaStr
   auto B_at = [&](int l) -> C* { return l == L ? leafB : Store<C>::Bm(P.ml[m][l]); };
   auto translate = [&](int lo, int hi, cudaStream_t st) {
     if (lo > hi) return;
-    if (P.tuning.m2l_variant >= 6) {
+    if (P.tuning.m2l_variant >= 6 && P.tuning.m2l_variant <= 8) {
       launch_m2l_grp<C>(
           P, lo, hi, P.tuning.m2l_variant == 6 ? 2 : 4, P.tuning.m2l_variant == 8, S_at, B_at,
           [&](int l) {

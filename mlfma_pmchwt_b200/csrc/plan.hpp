@@ -121,7 +121,8 @@ struct Tuning {
                                // 5: as 4 with the J and M halves on separate warps;
                                // 6: groups of 8 boxes, the union's source patterns staged in shared
                                //    memory by bulk asynchronous copies, 2 boxes per warp;
-                               // 7: as 6 with 4 boxes per warp
+                               // 7: as 6 with 4 boxes per warp; 8: as 7 with the source patterns
+                               //    by TMA tile copies
   int l2l_variant = 1;         // 0: 2-D transposed taps per child direction; 1: separable
   int up_variant = 0;          // 0: 9-tap gather per parent direction; 1: separable in bands;
                                // 2: 9-tap gather, all 6 components per thread;
