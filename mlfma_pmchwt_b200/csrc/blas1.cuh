@@ -223,5 +223,28 @@ inline void givens_apply(std::complex<double>& x, std::complex<double>& y, std::
   x = t;
 }
 
+// The same rotations on the device, for the inner GMRES steps that run
+// without a host round trip.
+__device__ __forceinline__ double2 dconj(double2 a) { return c2(a.x, -a.y); }
+__device__ inline void dgivens_make(double2 a, double2 b, double2& c, double2& s) {
+  const double eps = 1e-16;
+  if (sqrt(b.x * b.x + b.y * b.y) < eps) {
+    c = c2(1.0, 0.0);
+    s = c2(0.0, 0.0);
+  } else if (sqrt(a.x * a.x + a.y * a.y) < eps) {
+    c = c2(0.0, 0.0);
+    s = c2(1.0, 0.0);
+  } else {
+    const double r = sqrt(a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y);
+    c = c2(a.x / r, a.y / r);
+    s = c2(b.x / r, b.y / r);
+  }
+}
+__device__ inline void dgivens_apply(double2& x, double2& y, double2 c, double2 s) {
+  const double2 t = cadd(cmul(dconj(c), x), cmul(dconj(s), y));
+  y = cadd(cmul(c2(-s.x, -s.y), x), cmul(c, y));
+  x = t;
+}
+
 }  // namespace blas1
 }  // namespace mlfma

@@ -87,29 +87,6 @@ struct InnerDev {
   int* flags;   // [0] breakdown, [1] columns in use
 };
 
-__device__ __forceinline__ double2 dconj(double2 a) { return c2(a.x, -a.y); }
-
-// The rotations of Code/GMRES.h:22-48 (as blas1::givens_make / givens_apply).
-__device__ void dgivens_make(double2 a, double2 b, double2& c, double2& s) {
-  const double eps = 1e-16;
-  if (sqrt(b.x * b.x + b.y * b.y) < eps) {
-    c = c2(1.0, 0.0);
-    s = c2(0.0, 0.0);
-  } else if (sqrt(a.x * a.x + a.y * a.y) < eps) {
-    c = c2(0.0, 0.0);
-    s = c2(1.0, 0.0);
-  } else {
-    const double r = sqrt(a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y);
-    c = c2(a.x / r, a.y / r);
-    s = c2(b.x / r, b.y / r);
-  }
-}
-__device__ void dgivens_apply(double2& x, double2& y, double2 c, double2 s) {
-  const double2 t = cadd(cmul(dconj(c), x), cmul(dconj(s), y));
-  y = cadd(cmul(c2(-s.x, -s.y), x), cmul(c, y));
-  x = t;
-}
-
 // beta = ||v|| from the norm partials; g = (beta, 0, ...); flags cleared
 __global__ void inner_begin(const double2* partial, int nblk, InnerDev d, int inner) {
   double s = 0.0;
@@ -133,7 +110,7 @@ __global__ void inner_step(InnerDev d, int j, int ld) {
   for (int i = 0; i <= j; ++i) Hj[i] = cadd(d.h1[i], d.h2[i]);
   const double hn = sqrt(d.hn2[0].x);
   Hj[j + 1] = c2(hn, 0.0);
-  for (int i = 0; i < j; ++i) dgivens_apply(Hj[i], Hj[i + 1], d.cs[i], d.sn[i]);
+  for (int i = 0; i < j; ++i) blas1::dgivens_apply(Hj[i], Hj[i + 1], d.cs[i], d.sn[i]);
   d.flags[1] = j + 1;
   if (hn < 1e-14 * d.sc[0]) {
     d.flags[0] = 1;
@@ -141,10 +118,10 @@ __global__ void inner_step(InnerDev d, int j, int ld) {
     return;
   }
   d.sc[1] = 1.0 / hn;
-  dgivens_make(Hj[j], Hj[j + 1], d.cs[j], d.sn[j]);
-  dgivens_apply(Hj[j], Hj[j + 1], d.cs[j], d.sn[j]);
+  blas1::dgivens_make(Hj[j], Hj[j + 1], d.cs[j], d.sn[j]);
+  blas1::dgivens_apply(Hj[j], Hj[j + 1], d.cs[j], d.sn[j]);
   Hj[j + 1] = c2(0.0, 0.0);
-  dgivens_apply(d.g[j], d.g[j + 1], d.cs[j], d.sn[j]);
+  blas1::dgivens_apply(d.g[j], d.g[j + 1], d.cs[j], d.sn[j]);
 }
 
 // y = R^{-1} g over the columns in use (Code/GMRES.h:165-182); zero beyond

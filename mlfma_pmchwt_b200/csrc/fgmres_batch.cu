@@ -3,7 +3,10 @@
 // step costs one batched operator apply (leaf patterns and near-field
 // entries read once per group of right-hand sides, matvec_kernels.cu) and
 // one batched near-field product per inner step, and every Gram-Schmidt /
-// update step is one launch over all active systems with one host sync.
+// update step is one launch over all active systems. The outer Arnoldi step
+// takes one host sync (its Givens rotations and convergence test are on the
+// host); the preconditioner's inner steps keep their small GMRES state on
+// the device and take none.
 // Per system the iteration is exactly fgmres_solve's (fgmres.cu): the
 // reference's restarted GMRES (Code/GMRES.h:65-217) with CGS2 Arnoldi,
 // complex Givens rotations, true residual per cycle and its divergence
@@ -309,6 +312,84 @@ __global__ void __launch_bounds__(128) near_batch_box_kernel(NearBatchArg<Z> a) 
   }
 }
 
+// Device state of the preconditioner's inner GMRES for every lockstep
+// position: Hessenberg columns, rotations, rotated right-hand side,
+// breakdown flags. The inner steps update it with one thread per position
+// (the arithmetic of fgmres.cu's single-system inner_step), so they run
+// without a host round trip.
+struct InnerBatch {
+  double2* H;    // [R][ld * inner], column-major per position
+  double2* cs;   // [R][inner]
+  double2* sn;   // [R][inner]
+  double2* g;    // [R][ld]
+  double* beta;  // [R]
+  int* done;     // [R]
+  int ld, inner;
+};
+
+// beta_a = ||v_a|| from the reduced norms (hred[a * ldh]); alpha_a = 1 / beta_a;
+// g_a = (beta_a, 0, ...); columns in use m_a = 0
+__global__ void inner_begin_b(int Ra, const double2* hred, int ldh, InnerBatch S, double* alpha, int* m) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= Ra) return;
+  const double beta = sqrt(hred[static_cast<long long>(a) * ldh].x);
+  S.beta[a] = beta;
+  alpha[a] = beta > 0.0 ? 1.0 / beta : 0.0;
+  for (int i = 0; i < S.ld; ++i) S.g[static_cast<long long>(a) * S.ld + i] = c2(i == 0 ? beta : 0.0, 0.0);
+  S.done[a] = 0;
+  m[a] = 0;
+}
+
+// Column j of H_a from both Gram-Schmidt passes' coefficients (hred[a * ldh
+// + i] + hred[a * ldh + ldp + i]) and ||u_a||^2 (hred[a * ldh + 2 ldp]); its
+// rotations; alpha_a = scale of the next basis vector (0 after a breakdown).
+__global__ void inner_step_b(int Ra, int j, const double2* hred, int ldh, int ldp, InnerBatch S, double* alpha,
+                             int* m) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= Ra) return;
+  if (S.done[a]) {
+    alpha[a] = 0.0;
+    return;
+  }
+  const double2* h = hred + static_cast<long long>(a) * ldh;
+  double2* Hj = S.H + (static_cast<long long>(a) * S.inner + j) * S.ld;
+  double2* cs = S.cs + static_cast<long long>(a) * S.inner;
+  double2* sn = S.sn + static_cast<long long>(a) * S.inner;
+  double2* g = S.g + static_cast<long long>(a) * S.ld;
+  for (int i = 0; i <= j; ++i) Hj[i] = cadd(h[i], h[ldp + i]);
+  const double hn = sqrt(h[2 * ldp].x);
+  Hj[j + 1] = c2(hn, 0.0);
+  for (int i = 0; i < j; ++i) blas1::dgivens_apply(Hj[i], Hj[i + 1], cs[i], sn[i]);
+  m[a] = j + 1;
+  if (hn < 1e-14 * S.beta[a]) {
+    S.done[a] = 1;
+    alpha[a] = 0.0;
+    return;
+  }
+  alpha[a] = 1.0 / hn;
+  blas1::dgivens_make(Hj[j], Hj[j + 1], cs[j], sn[j]);
+  blas1::dgivens_apply(Hj[j], Hj[j + 1], cs[j], sn[j]);
+  Hj[j + 1] = c2(0.0, 0.0);
+  blas1::dgivens_apply(g[j], g[j + 1], cs[j], sn[j]);
+}
+
+// y_a = R_a^{-1} g_a over the m_a columns in use (Code/GMRES.h:165-182)
+__global__ void inner_end_b(int Ra, InnerBatch S, const int* m, double2* y, int ldy) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= Ra) return;
+  const double eps = 1e-16;
+  const int ma = m[a];
+  const double2* H = S.H + static_cast<long long>(a) * S.inner * S.ld;
+  const double2* g = S.g + static_cast<long long>(a) * S.ld;
+  double2* ya = y + static_cast<long long>(a) * ldy;
+  for (int i = ma - 1; i >= 0; --i) {
+    double2 yi = g[i];
+    for (int j = i + 1; j < ma; ++j) yi = csub(yi, cmul(H[i + static_cast<long long>(j) * S.ld], ya[j]));
+    const double2 hii = H[i + static_cast<long long>(i) * S.ld];
+    ya[i] = sqrt(hii.x * hii.x + hii.y * hii.y) > eps ? cdiv(yi, hii) : c2(0.0, 0.0);
+  }
+}
+
 // Upper-triangular solve of the rotated least-squares system (Code/GMRES.h:165-182).
 void back_substitute(const std::vector<C>& H, int ld, const std::vector<C>& s, int m, std::vector<C>& y) {
   const double eps = 1e-16;
@@ -338,10 +419,15 @@ struct BatchOps {
 
   dim3 grid(int Ra) const { return dim3(nblk, Ra); }
 
-  // norms of the operand (or of b - w, writing r) for Ra positions
-  std::vector<double> norms(int Ra, const int* sys, VecRef w, VecRef b = {}, VecRef r = {}, bool has_b = false) {
+  // squared norms of the operand (or of b - w, writing r) for Ra positions,
+  // left on the device at hdev[a * (2 ldp + 2)]
+  void norms_dev(int Ra, const int* sys, VecRef w, VecRef b = {}, VecRef r = {}, bool has_b = false) {
     norm_b<<<grid(Ra), kBT, 0, s>>>(b, w, r, sys, n, has_b ? 1 : 0, part, ldp);
     reduce_b<<<dim3(1, Ra), 32, 0, s>>>(part, nblk, ldp, 1, hdev, 2 * ldp + 2);
+  }
+  // norms of the operand (or of b - w, writing r) for Ra positions
+  std::vector<double> norms(int Ra, const int* sys, VecRef w, VecRef b = {}, VecRef r = {}, bool has_b = false) {
+    norms_dev(Ra, sys, w, b, r, has_b);
     hbuf.resize(static_cast<size_t>(Ra) * (2 * ldp + 2));
     MLFMA_CUDA(cudaMemcpyAsync(hbuf.data(), hdev, hbuf.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
     MLFMA_CUDA(cudaStreamSynchronize(s));
@@ -350,8 +436,9 @@ struct BatchOps {
     return out;
   }
   // CGS2 of w_a against V_a[0..nv): hcol[a][j] and ||w_a|| after projection
-  void orthogonalise(int Ra, const int* sys, VecRef V, VecRef w, int nv, std::vector<std::vector<C>>& hcol,
-                     std::vector<double>& hn) {
+  // CGS2 launches only: per position a, hdev[a * ldh + j] and [a * ldh + ldp
+  // + j] the two passes' coefficients, [a * ldh + 2 ldp] ||w_a||^2 after them
+  void orthogonalise_dev(int Ra, const int* sys, VecRef V, VecRef w, int nv) {
     const int ldh = 2 * ldp + 2;
     dots_b<<<grid(Ra), kBT, 0, s>>>(V, w, sys, n, nv, part, ldp);
     reduce_b<<<dim3(1, Ra), 64, 0, s>>>(part, nblk, ldp, nv, hdev, ldh);
@@ -360,6 +447,11 @@ struct BatchOps {
     reduce_b<<<dim3(1, Ra), 64, 0, s>>>(part, nblk, ldp, nv, hdev + ldp, ldh);
     project_b<<<grid(Ra), kBT, 0, s>>>(V, w, sys, n, nv, hdev + ldp, ldh, 1, part, ldp);
     reduce_b<<<dim3(1, Ra), 32, 0, s>>>(part, nblk, ldp, 1, hdev + 2 * ldp, ldh);
+  }
+  void orthogonalise(int Ra, const int* sys, VecRef V, VecRef w, int nv, std::vector<std::vector<C>>& hcol,
+                     std::vector<double>& hn) {
+    const int ldh = 2 * ldp + 2;
+    orthogonalise_dev(Ra, sys, V, w, nv);
     hbuf.resize(static_cast<size_t>(Ra) * ldh);
     MLFMA_CUDA(cudaMemcpyAsync(hbuf.data(), hdev, hbuf.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
     MLFMA_CUDA(cudaStreamSynchronize(s));
@@ -403,35 +495,30 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   reserve_batch(P, R);
   cudaStream_t s = P.stream;
   const long long n = 2LL * P.N;
-  blas1::Work g;
+  // work arrays from the plan's arena: no allocation when the last call's fit
+  P.arena.reset();
+  auto get = [&](size_t count) { return static_cast<double2*>(P.arena.get(count * sizeof(double2))); };
   const int ldp = blas1::kMaxBasis + 2;
   const long long vs = static_cast<long long>(mr + 1) * n;       // per-system basis stride
   const long long zs = static_cast<long long>(mr) * n;
   const long long qs = static_cast<long long>(inner_its + 1) * n;
-  double2* x = g.get(static_cast<size_t>(R) * n);
-  double2* b = g.get(static_cast<size_t>(R) * n);
-  double2* r = g.get(static_cast<size_t>(R) * n);
-  double2* V = g.get(static_cast<size_t>(R) * vs);
-  double2* Zd = inner_its > 0 ? g.get(static_cast<size_t>(R) * zs) : nullptr;
-  double2* Q = inner_its > 0 ? g.get(static_cast<size_t>(R) * qs) : nullptr;
+  double2* x = get(static_cast<size_t>(R) * n);
+  double2* b = get(static_cast<size_t>(R) * n);
+  double2* r = get(static_cast<size_t>(R) * n);
+  double2* V = get(static_cast<size_t>(R) * vs);
+  double2* Zd = inner_its > 0 ? get(static_cast<size_t>(R) * zs) : nullptr;
+  double2* Q = inner_its > 0 ? get(static_cast<size_t>(R) * qs) : nullptr;
   const int G = std::min(R, kBatchSlots);  // staging rows: one batched apply at a time
-  double2* Xs = g.get(static_cast<size_t>(G) * n);
-  double2* Ws = g.get(static_cast<size_t>(G) * n);
+  double2* Xs = get(static_cast<size_t>(G) * n);
+  double2* Ws = get(static_cast<size_t>(G) * n);
   const int nblk = std::max(1, blas1::kBlocks / std::min(R, 8));
   BatchOps ops{s, n, nblk, ldp};
-  ops.part = g.get(static_cast<size_t>(R) * nblk * ldp);
-  ops.hdev = g.get(static_cast<size_t>(R) * (2 * ldp + 2));
-  void* tmp = nullptr;
-  MLFMA_CUDA(cudaMalloc(&tmp, static_cast<size_t>(R) * sizeof(double)));
-  g.owned.push_back(tmp);
-  ops.alpha = static_cast<double*>(tmp);
-  MLFMA_CUDA(cudaMalloc(&tmp, static_cast<size_t>(R) * sizeof(int)));
-  g.owned.push_back(tmp);
-  ops.mdev = static_cast<int*>(tmp);
-  ops.ydev = g.get(static_cast<size_t>(R) * blas1::kMaxBasis);
-  MLFMA_CUDA(cudaMalloc(&tmp, static_cast<size_t>(R) * sizeof(int)));
-  g.owned.push_back(tmp);
-  int* sysd = static_cast<int*>(tmp);
+  ops.part = get(static_cast<size_t>(R) * nblk * ldp);
+  ops.hdev = get(static_cast<size_t>(R) * (2 * ldp + 2));
+  ops.alpha = reinterpret_cast<double*>(get(R));
+  ops.mdev = reinterpret_cast<int*>(get(R));
+  ops.ydev = get(static_cast<size_t>(R) * blas1::kMaxBasis);
+  int* sysd = reinterpret_cast<int*>(get(R));
   MLFMA_CUDA(cudaMemcpyAsync(x, xh, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyHostToDevice, s));
   MLFMA_CUDA(cudaMemcpyAsync(b, rhs, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyHostToDevice, s));
   st.assign(R, SolveStats());
@@ -481,22 +568,28 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   if (inner_its > 0 && box_smem <= kNearBoxSmemMax)
     MLFMA_CUDA(cudaFuncSetAttribute(near_batch_box_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kNearBoxSmemMax)));
-  // z_q = (inner_its GMRES steps on Z_near from zero) applied to v_q, q in list
+  // inner GMRES state on the device (one row per lockstep position)
+  InnerBatch ib{};
+  if (inner_its > 0) {
+    ib.ld = inner_its + 1;
+    ib.inner = inner_its;
+    ib.H = get(static_cast<size_t>(R) * ib.ld * inner_its);
+    ib.cs = get(static_cast<size_t>(R) * inner_its);
+    ib.sn = get(static_cast<size_t>(R) * inner_its);
+    ib.g = get(static_cast<size_t>(R) * ib.ld);
+    ib.beta = reinterpret_cast<double*>(get(R));
+    ib.done = reinterpret_cast<int*>(get(R));
+  }
+  const int ldh = 2 * ldp + 2;
+  // z_q = (inner_its GMRES steps on Z_near from zero) applied to v_q, q in
+  // list: every step is launches only, the host waits for none of them
   auto precondition = [&](const std::vector<int>& list, long long voff, long long zoff) {
     const int Ra = static_cast<int>(list.size());
+    const int pb = (Ra + 63) / 64;
     set_sys(list);
-    const std::vector<double> beta = ops.norms(Ra, sysd, sysref(V, vs, voff));
-    std::vector<double> inv(Ra);
-    for (int a = 0; a < Ra; ++a) inv[a] = beta[a] > 0 ? 1.0 / beta[a] : 0.0;
-    ops.scale(Ra, sysd, sysref(V, vs, voff), sysref(Q, qs, 0), inv);
-    const int ld = inner_its + 1;
-    std::vector<std::vector<C>> Hi(Ra, std::vector<C>(static_cast<size_t>(ld) * inner_its, C(0.0)));
-    std::vector<std::vector<C>> ci(Ra, std::vector<C>(ld)), si(Ra, std::vector<C>(ld)), gi(Ra, std::vector<C>(ld));
-    std::vector<int> used(Ra, 0);
-    std::vector<char> done(Ra, 0);
-    for (int a = 0; a < Ra; ++a) gi[a][0] = beta[a];
-    std::vector<std::vector<C>> hcol;
-    std::vector<double> hn;
+    ops.norms_dev(Ra, sysd, sysref(V, vs, voff));
+    inner_begin_b<<<pb, 64, 0, s>>>(Ra, ops.hdev, ldh, ib, ops.alpha, ops.mdev);
+    scale_b<<<ops.grid(Ra), kBT, 0, s>>>(sysref(V, vs, voff), sysref(Q, qs, 0), sysd, n, ops.alpha);
     for (int j = 0; j < inner_its; ++j) {
       {  // the preconditioner's near field is the complex64 copy at either precision
         NearBatchArg<float2> na{P.d_leaf_rwg,  P.d_rwg_leafbox,      P.d_leaf_ptr,
@@ -511,32 +604,16 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
           near_batch_kernel<float2><<<ng, 128, 0, s>>>(na);
         }
       }
-      MLFMA_CUDA(cudaGetLastError());
       for (int q : list) st[q].near_products++;
-      ops.orthogonalise(Ra, sysd, sysref(Q, qs, 0), sysref(Q, qs, (j + 1) * n), j + 1, hcol, hn);
-      std::vector<double> sc(Ra, 1.0);
-      for (int a = 0; a < Ra; ++a) {
-        if (done[a]) continue;
-        std::vector<C>& H = Hi[a];
-        for (int i = 0; i <= j; ++i) H[i + j * ld] = hcol[a][i];
-        H[j + 1 + j * ld] = hn[a];
-        used[a] = j + 1;
-        if (hn[a] < 1e-14 * beta[a]) {
-          done[a] = 1;
-          continue;
-        }
-        sc[a] = 1.0 / hn[a];
-        for (int i = 0; i < j; ++i) blas1::givens_apply(H[i + j * ld], H[i + 1 + j * ld], ci[a][i], si[a][i]);
-        blas1::givens_make(H[j + j * ld], H[j + 1 + j * ld], ci[a][j], si[a][j]);
-        blas1::givens_apply(H[j + j * ld], H[j + 1 + j * ld], ci[a][j], si[a][j]);
-        H[j + 1 + j * ld] = C(0.0);
-        blas1::givens_apply(gi[a][j], gi[a][j + 1], ci[a][j], si[a][j]);
-      }
-      ops.scale(Ra, sysd, sysref(Q, qs, (j + 1) * n), sysref(Q, qs, (j + 1) * n), sc);
+      ops.orthogonalise_dev(Ra, sysd, sysref(Q, qs, 0), sysref(Q, qs, (j + 1) * n), j + 1);
+      inner_step_b<<<pb, 64, 0, s>>>(Ra, j, ops.hdev, ldh, ldp, ib, ops.alpha, ops.mdev);
+      scale_b<<<ops.grid(Ra), kBT, 0, s>>>(sysref(Q, qs, (j + 1) * n), sysref(Q, qs, (j + 1) * n), sysd, n,
+                                           ops.alpha);
     }
-    std::vector<std::vector<C>> y(Ra);
-    for (int a = 0; a < Ra; ++a) back_substitute(Hi[a], ld, gi[a], used[a], y[a]);
-    ops.combine(Ra, sysd, sysref(Q, qs, 0), sysref(Zd, zs, zoff), y, false);
+    inner_end_b<<<pb, 64, 0, s>>>(Ra, ib, ops.mdev, ops.ydev, blas1::kMaxBasis);
+    combine_b<<<ops.grid(Ra), kBT, 0, s>>>(sysref(Q, qs, 0), sysref(Zd, zs, zoff), sysd, n, ops.mdev, ops.ydev,
+                                           blas1::kMaxBasis, 0);
+    MLFMA_CUDA(cudaGetLastError());
     // a learned correction of each z, when a network is attached to the plan
     if (const __nv_bfloat16* wl = lp_attached(P))
       for (int q : list) lp_forward(P, wl, V + q * vs + voff, Zd + q * zs + zoff, Zd + q * zs + zoff, false, s);
@@ -659,6 +736,7 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   }
   MLFMA_CUDA(cudaMemcpyAsync(xh, x, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyDeviceToHost, s));
   MLFMA_CUDA(cudaStreamSynchronize(s));
+  if (P.arena.total() > Plan::SolveArena::kKeepBytes) P.arena.release();
   seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   for (int q = 0; q < R; ++q) {
     st[q].seconds = seconds;

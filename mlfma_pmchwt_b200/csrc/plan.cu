@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <map>
+#include <new>
 
 #include "cplx.cuh"
 #include "near_same_triangle.hpp"
@@ -16,6 +17,43 @@ void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+void* Plan::SolveArena::get(size_t bytes) {
+  if (bytes == 0) bytes = 1;
+  bytes = (bytes + 255) & ~size_t(255);
+  if (next == ptr.size()) {
+    ptr.push_back(nullptr);
+    cap.push_back(0);
+  }
+  if (cap[next] < bytes) {
+    if (ptr[next]) check_cuda(cudaFree(ptr[next]), "cudaFree");
+    ptr[next] = nullptr;
+    cap[next] = 0;
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw std::bad_alloc();
+    }
+    ptr[next] = p;
+    cap[next] = bytes;
+  }
+  return ptr[next++];
+}
+
+size_t Plan::SolveArena::total() const {
+  size_t t = 0;
+  for (size_t c : cap) t += c;
+  return t;
+}
+
+void Plan::SolveArena::release() {
+  for (void* p : ptr)
+    if (p) cudaFree(p);
+  ptr.clear();
+  cap.clear();
+  next = 0;
+}
+
 Plan::~Plan() {
   if (device >= 0) {
     cudaSetDevice(device);
@@ -24,6 +62,7 @@ Plan::~Plan() {
     for (auto& set : prof.sets)
       for (cudaEvent_t e : set) cudaEventDestroy(e);
     for (void* p : allocations) cudaFree(p);
+    arena.release();
     if (h_status) cudaFreeHost(h_status);
     if (stream) cudaStreamDestroy(stream);
     if (stream2) {

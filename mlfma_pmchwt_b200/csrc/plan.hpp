@@ -249,6 +249,20 @@ struct Plan {
   std::shared_ptr<LearnedWork> lp;  // allocated on first use; its device arrays are in allocations
   size_t bytes = 0;
   std::vector<void*> allocations;
+  // Device work arrays of the lockstep solve, kept from one call to the next:
+  // call k's i-th request reuses slot i (reallocated when too small), so a
+  // refinement's repeated solves and solve after solve allocate nothing.
+  // Freed with the plan, or at the end of a call when they exceed kKeepBytes.
+  struct SolveArena {
+    static constexpr size_t kKeepBytes = size_t(16) << 30;
+    std::vector<void*> ptr;
+    std::vector<size_t> cap;
+    size_t next = 0;
+    void* get(size_t bytes);
+    void reset() { next = 0; }
+    size_t total() const;
+    void release();
+  } arena;
 
   ~Plan();
   void tf_inputs(int m, int l, std::vector<double>& rhat, std::vector<int>& hoff, std::vector<int>& hL,
