@@ -213,12 +213,8 @@ int mlfma_apply_batch(mlfma_plan* plan, int n, int R, const double* x, double* w
   return guarded([&] {
     mlfma::Plan& P = *plan->p;
     MLFMA_CUDA(cudaSetDevice(P.device));
-    mlfma::reserve_batch(P, R);
-    if (P.xb_cap == 0) {
-      P.d_xb = P.alloc<double2>(static_cast<size_t>(mlfma::kBatchSlots) * n);
-      P.d_wb = P.alloc<double2>(static_cast<size_t>(mlfma::kBatchSlots) * n);
-      P.xb_cap = mlfma::kBatchSlots;
-    }
+    mlfma::reserve_batch(P, R, true);
+    mlfma::reserve_batch_staging(P);
     for (int g0 = 0; g0 < R; g0 += P.xb_cap) {
       const int rn = std::min(P.xb_cap, R - g0);
       const size_t bytes = static_cast<size_t>(rn) * n * sizeof(double2);
@@ -242,7 +238,7 @@ int mlfma_apply_batch_device(mlfma_plan* plan, int n, int R, const void* x_dev, 
   return guarded([&] {
     mlfma::Plan& P = *plan->p;
     MLFMA_CUDA(cudaSetDevice(P.device));
-    mlfma::reserve_batch(P, R);
+    mlfma::reserve_batch(P, R, true);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
     mlfma::apply_batch_device(P, R, static_cast<const double2*>(x_dev), n, static_cast<double2*>(w_dev), n, s);
     return MLFMA_OK;
@@ -259,7 +255,7 @@ int mlfma_apply_batch_mixed_device(mlfma_plan* plan, int n, int R, const void* x
   return guarded([&] {
     mlfma::Plan& P = *plan->p;
     MLFMA_CUDA(cudaSetDevice(P.device));
-    mlfma::reserve_batch(P, R);
+    mlfma::reserve_batch(P, R, false);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : P.stream;
     mlfma::apply_batch_mixed_device(P, R, static_cast<const double2*>(x_dev), n, static_cast<double2*>(w_dev), n, s);
     return MLFMA_OK;

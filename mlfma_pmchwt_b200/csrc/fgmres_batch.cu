@@ -492,33 +492,49 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   if (inner_its < 0 || inner_its + 1 > blas1::kMaxBasis) throw std::invalid_argument("inner_its must be in 0..63");
   const auto t0 = std::chrono::steady_clock::now();
   MLFMA_CUDA(cudaSetDevice(P.device));
-  reserve_batch(P, R);
+  reserve_batch(P, R, false);
   cudaStream_t s = P.stream;
   const long long n = 2LL * P.N;
-  // work arrays from the plan's arena: no allocation when the last call's fit
-  P.arena.reset();
-  auto get = [&](size_t count) { return static_cast<double2*>(P.arena.get(count * sizeof(double2))); };
   const int ldp = blas1::kMaxBasis + 2;
   const long long vs = static_cast<long long>(mr + 1) * n;       // per-system basis stride
   const long long zs = static_cast<long long>(mr) * n;
   const long long qs = static_cast<long long>(inner_its + 1) * n;
-  double2* x = get(static_cast<size_t>(R) * n);
-  double2* b = get(static_cast<size_t>(R) * n);
-  double2* r = get(static_cast<size_t>(R) * n);
-  double2* V = get(static_cast<size_t>(R) * vs);
-  double2* Zd = inner_its > 0 ? get(static_cast<size_t>(R) * zs) : nullptr;
-  double2* Q = inner_its > 0 ? get(static_cast<size_t>(R) * qs) : nullptr;
   const int G = std::min(R, kBatchSlots);  // staging rows: one batched apply at a time
-  double2* Xs = get(static_cast<size_t>(G) * n);
-  double2* Ws = get(static_cast<size_t>(G) * n);
   const int nblk = std::max(1, blas1::kBlocks / std::min(R, 8));
+  const int ldi = inner_its + 1;
+  const size_t Rz = static_cast<size_t>(R);
+  // work arrays (counts of complex128 values), in one block of the plan's
+  // arena: no allocation when the last call's block is large enough
+  enum { kX, kB, kR, kV, kZ, kQ, kXs, kWs, kPart, kH, kAlpha, kM, kY, kSys, kIH, kICs, kISn, kIG, kIBeta, kIDone, kN };
+  const size_t cnt[kN] = {Rz * n, Rz * n, Rz * n, Rz * vs, inner_its > 0 ? Rz * zs : 0, inner_its > 0 ? Rz * qs : 0,
+                          static_cast<size_t>(G) * n, static_cast<size_t>(G) * n, Rz * nblk * ldp,
+                          Rz * (2 * ldp + 2), Rz, Rz, Rz * blas1::kMaxBasis, Rz,
+                          inner_its > 0 ? Rz * ldi * inner_its : 0, Rz * inner_its, Rz * inner_its, Rz * ldi, Rz, Rz};
+  size_t work_bytes = 0;
+  for (size_t c : cnt) work_bytes += (c * sizeof(double2) + 255) & ~size_t(255);
+  P.arena.reserve(work_bytes);
+  double2* wk[kN];
+  for (int i = 0; i < kN; ++i) wk[i] = cnt[i] ? static_cast<double2*>(P.arena.get(cnt[i] * sizeof(double2))) : nullptr;
+  double2 *x = wk[kX], *b = wk[kB], *r = wk[kR], *V = wk[kV], *Zd = wk[kZ], *Q = wk[kQ], *Xs = wk[kXs], *Ws = wk[kWs];
   BatchOps ops{s, n, nblk, ldp};
-  ops.part = get(static_cast<size_t>(R) * nblk * ldp);
-  ops.hdev = get(static_cast<size_t>(R) * (2 * ldp + 2));
-  ops.alpha = reinterpret_cast<double*>(get(R));
-  ops.mdev = reinterpret_cast<int*>(get(R));
-  ops.ydev = get(static_cast<size_t>(R) * blas1::kMaxBasis);
-  int* sysd = reinterpret_cast<int*>(get(R));
+  ops.part = wk[kPart];
+  ops.hdev = wk[kH];
+  ops.alpha = reinterpret_cast<double*>(wk[kAlpha]);
+  ops.mdev = reinterpret_cast<int*>(wk[kM]);
+  ops.ydev = wk[kY];
+  int* sysd = reinterpret_cast<int*>(wk[kSys]);
+  // inner GMRES state on the device (one row per lockstep position)
+  InnerBatch ib{};
+  if (inner_its > 0) {
+    ib.ld = ldi;
+    ib.inner = inner_its;
+    ib.H = wk[kIH];
+    ib.cs = wk[kICs];
+    ib.sn = wk[kISn];
+    ib.g = wk[kIG];
+    ib.beta = reinterpret_cast<double*>(wk[kIBeta]);
+    ib.done = reinterpret_cast<int*>(wk[kIDone]);
+  }
   MLFMA_CUDA(cudaMemcpyAsync(x, xh, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyHostToDevice, s));
   MLFMA_CUDA(cudaMemcpyAsync(b, rhs, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyHostToDevice, s));
   st.assign(R, SolveStats());
@@ -568,18 +584,6 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   if (inner_its > 0 && box_smem <= kNearBoxSmemMax)
     MLFMA_CUDA(cudaFuncSetAttribute(near_batch_box_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kNearBoxSmemMax)));
-  // inner GMRES state on the device (one row per lockstep position)
-  InnerBatch ib{};
-  if (inner_its > 0) {
-    ib.ld = inner_its + 1;
-    ib.inner = inner_its;
-    ib.H = get(static_cast<size_t>(R) * ib.ld * inner_its);
-    ib.cs = get(static_cast<size_t>(R) * inner_its);
-    ib.sn = get(static_cast<size_t>(R) * inner_its);
-    ib.g = get(static_cast<size_t>(R) * ib.ld);
-    ib.beta = reinterpret_cast<double*>(get(R));
-    ib.done = reinterpret_cast<int*>(get(R));
-  }
   const int ldh = 2 * ldp + 2;
   // z_q = (inner_its GMRES steps on Z_near from zero) applied to v_q, q in
   // list: every step is launches only, the host waits for none of them
@@ -736,7 +740,7 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   }
   MLFMA_CUDA(cudaMemcpyAsync(xh, x, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyDeviceToHost, s));
   MLFMA_CUDA(cudaStreamSynchronize(s));
-  if (P.arena.total() > Plan::SolveArena::kKeepBytes) P.arena.release();
+  if (P.arena.cap > Plan::SolveArena::kKeepBytes) P.arena.release();
   seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   for (int q = 0; q < R; ++q) {
     st[q].seconds = seconds;

@@ -1794,7 +1794,8 @@ void apply_fixed(Plan& P, const double2* x, double2* w, cudaStream_t s) {
 template <class C>
 void apply_batch_fixed(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw, cudaStream_t s) {
   const int L = P.maxL;
-  if (P.batch_cap < std::min(R, kBatchSlots)) throw std::runtime_error("batched apply: slots not reserved");
+  if (std::is_same<C, float2>::value ? P.bS32[0].empty() : P.batch_cap < std::min(R, kBatchSlots))
+    throw std::runtime_error("batched apply: slots not reserved");
   constexpr int kAggRB = 8, kLeafRB = 4;
   for (int g0 = 0; g0 < R; g0 += kBatchSlots) {
     const int rn = std::min(kBatchSlots, R - g0);
@@ -1972,16 +1973,29 @@ void apply_direct(Plan& P, const double2* x, double2* w, cudaStream_t s) {
   if (ev) MLFMA_CUDA(cudaEventRecord(ev[9], s));
 }
 
-void reserve_batch(Plan& P, int R) {
+void reserve_batch_staging(Plan& P) {
+  if (P.xb_cap > 0) return;
+  P.d_xb = P.alloc<double2>(static_cast<size_t>(kBatchSlots) * 2 * P.N);
+  P.d_wb = P.alloc<double2>(static_cast<size_t>(kBatchSlots) * 2 * P.N);
+  P.xb_cap = kBatchSlots;
+}
+
+void reserve_batch(Plan& P, int R, bool fp64) {
   const int want = std::min(R, kBatchSlots);
   const int L = P.maxL;
   if (P.precision == 1 && P.bS32[0].empty()) {
-    // the complex64 tree of every slot at once, slot-major per level
+    // the complex64 tree of every slot at once, slot-major per level, in one
+    // allocation
+    size_t total = 0;
+    for (int m = 0; m < 2; ++m)
+      for (int l = 2; l <= L; ++l) total += 2 * kBatchSlots * static_cast<size_t>(P.lv[l].B) * 6 * P.ml[m][l].K;
+    float2* p = P.alloc<float2>(total);
     for (int m = 0; m < 2; ++m) {
       for (int l = 2; l <= L; ++l) {
         const size_t cnt = static_cast<size_t>(P.lv[l].B) * 6 * P.ml[m][l].K;
-        P.btS[m][l] = P.alloc<float2>(kBatchSlots * cnt);
-        P.btB[m][l] = P.alloc<float2>(kBatchSlots * cnt);
+        P.btS[m][l] = p;
+        P.btB[m][l] = p + kBatchSlots * cnt;
+        p += 2 * kBatchSlots * cnt;
       }
       const size_t cnt = static_cast<size_t>(P.lv[L].B) * 6 * P.ml[m][L].K;
       for (int j = 0; j < kBatchSlots; ++j) {
@@ -1990,13 +2004,21 @@ void reserve_batch(Plan& P, int R) {
       }
     }
   }
-  while (P.batch_cap < want) {
+  if (fp64 && P.batch_cap < want) {
+    // the FP64 leaf arrays of the slots still missing, in one allocation
+    const int add = want - P.batch_cap;
+    size_t total = 0;
+    for (int m = 0; m < 2; ++m) total += 2 * static_cast<size_t>(add) * P.lv[L].B * 6 * P.ml[m][L].K;
+    double2* p = P.alloc<double2>(total);
     for (int m = 0; m < 2; ++m) {
       const size_t cnt = static_cast<size_t>(P.lv[L].B) * 6 * P.ml[m][L].K;
-      P.bS[m].push_back(P.alloc<double2>(cnt));
-      P.bB[m].push_back(P.alloc<double2>(cnt));
+      for (int j = 0; j < add; ++j) {
+        P.bS[m].push_back(p);
+        P.bB[m].push_back(p + cnt);
+        p += 2 * cnt;
+      }
     }
-    ++P.batch_cap;
+    P.batch_cap = want;
   }
 }
 

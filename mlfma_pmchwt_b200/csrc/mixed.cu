@@ -137,14 +137,13 @@ std::vector<char> mixed_batch_solve(Plan& P, int R, double* xh, const double* rh
   if (refine_max < 0) throw std::invalid_argument("refine_max must be non-negative");
   const auto t0 = std::chrono::steady_clock::now();
   MLFMA_CUDA(cudaSetDevice(P.device));
-  reserve_batch(P, R);
+  reserve_batch(P, R, false);
+  reserve_batch_staging(P);  // the FP64 residuals' device rows
   const long long n = 2LL * P.N;
   C* X = reinterpret_cast<C*>(xh);
   const C* B = reinterpret_cast<const C*>(rhs);
-  blas1::Work g;
-  const int G = std::min(R, kBatchSlots);
-  double2* Xd = g.get(static_cast<size_t>(G) * n);
-  double2* Wd = g.get(static_cast<size_t>(G) * n);
+  double2* Xd = P.d_xb;
+  double2* Wd = P.d_wb;
   std::vector<C> Rr(static_cast<size_t>(R) * n);
   st.assign(R, SolveStats());
   std::vector<double> bnorm(R), err(R);

@@ -5,7 +5,6 @@
 #include <cmath>
 #include <cstdio>
 #include <map>
-#include <new>
 
 #include "cplx.cuh"
 #include "near_same_triangle.hpp"
@@ -17,51 +16,78 @@ void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-void* Plan::SolveArena::get(size_t bytes) {
-  if (bytes == 0) bytes = 1;
-  bytes = (bytes + 255) & ~size_t(255);
-  if (next == ptr.size()) {
-    ptr.push_back(nullptr);
-    cap.push_back(0);
+
+namespace {
+constexpr size_t kAlign = 256;
+size_t round_up(size_t b) { return (b + kAlign - 1) & ~(kAlign - 1); }
+void* device_block(size_t bytes) {
+  void* p = nullptr;
+  const cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw std::runtime_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
   }
-  if (cap[next] < bytes) {
-    if (ptr[next]) check_cuda(cudaFree(ptr[next]), "cudaFree");
-    ptr[next] = nullptr;
-    cap[next] = 0;
-    void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      throw std::bad_alloc();
-    }
-    ptr[next] = p;
-    cap[next] = bytes;
+  return p;
+}
+}  // namespace
+
+void* Plan::DeviceHeap::get(size_t bytes) {
+  bytes = round_up(bytes ? bytes : 1);
+  if (bytes > kChunk / 4) {
+    blocks.push_back(device_block(bytes));
+    return blocks.back();
   }
-  return ptr[next++];
+  if (bytes > left) {
+    blocks.push_back(device_block(kChunk));
+    cur = static_cast<char*>(blocks.back());
+    left = kChunk;
+  }
+  void* p = cur;
+  cur += bytes;
+  left -= bytes;
+  return p;
 }
 
-size_t Plan::SolveArena::total() const {
-  size_t t = 0;
-  for (size_t c : cap) t += c;
-  return t;
+void Plan::DeviceHeap::release() {
+  for (void* p : blocks) cudaFree(p);
+  blocks.clear();
+  cur = nullptr;
+  left = 0;
+}
+
+void Plan::SolveArena::reserve(size_t bytes) {
+  if (bytes > cap) {
+    release();
+    base = static_cast<char*>(device_block(bytes));
+    cap = bytes;
+  }
+  used = 0;
+}
+
+void* Plan::SolveArena::get(size_t bytes) {
+  bytes = round_up(bytes ? bytes : 1);
+  if (used + bytes > cap) throw std::logic_error("solve arena: request beyond the reservation");
+  void* p = base + used;
+  used += bytes;
+  return p;
 }
 
 void Plan::SolveArena::release() {
-  for (void* p : ptr)
-    if (p) cudaFree(p);
-  ptr.clear();
-  cap.clear();
-  next = 0;
+  if (base) cudaFree(base);
+  base = nullptr;
+  cap = used = 0;
 }
 
 Plan::~Plan() {
   if (device >= 0) {
     cudaSetDevice(device);
-    if (stream) cudaStreamSynchronize(stream);
+    // every stream of the plan idle before its memory goes back
+    for (cudaStream_t st : {stream, stream2, stream_near, stream_leaf[0], stream_leaf[1]})
+      if (st) cudaStreamSynchronize(st);
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     for (auto& set : prof.sets)
       for (cudaEvent_t e : set) cudaEventDestroy(e);
-    for (void* p : allocations) cudaFree(p);
+    heap.release();
     arena.release();
     if (h_status) cudaFreeHost(h_status);
     if (stream) cudaStreamDestroy(stream);
@@ -499,7 +525,7 @@ std::unique_ptr<Plan> create_plan(Mesh&& mesh, const PlanParams& prm) {
         std::vector<double2> h2all;
         P->tf_inputs(m, l, rhat, hoff, hL, h2all);
         M.tfw = P->alloc<double2>(static_cast<size_t>(std::max(M.nvec, 1)) * M.K);
-        launch_transfer(*P, m, l, rhat, hoff, hL, h2all, true, M.tfw, s);
+        launch_transfer(*P, m, l, rhat, hoff, hL, h2all, true, M.tfw, s, true);
       }
     }
   }

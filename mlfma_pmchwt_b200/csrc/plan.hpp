@@ -246,21 +246,31 @@ struct Plan {
   cudaEvent_t ev_start = nullptr, ev_near = nullptr;
   StageProfiler prof;
   std::vector<ApplyGraph> graphs;
-  std::shared_ptr<LearnedWork> lp;  // allocated on first use; its device arrays are in allocations
+  std::shared_ptr<LearnedWork> lp;  // allocated on first use; its device arrays are in the heap
   size_t bytes = 0;
-  std::vector<void*> allocations;
-  // Device work arrays of the lockstep solve, kept from one call to the next:
-  // call k's i-th request reuses slot i (reallocated when too small), so a
-  // refinement's repeated solves and solve after solve allocate nothing.
-  // Freed with the plan, or at the end of a call when they exceed kKeepBytes.
+  // Plan-lifetime device memory, carved (256-byte aligned) from chunks of
+  // kChunk bytes: one driver allocation per chunk instead of one per array
+  // (a driver allocation costs milliseconds, and far more on a busy node);
+  // requests above kChunk / 4 get their own. Nothing goes back before the
+  // plan is destroyed, so no array ever shares memory with a freed one.
+  struct DeviceHeap {
+    static constexpr size_t kChunk = size_t(64) << 20;
+    std::vector<void*> blocks;
+    char* cur = nullptr;
+    size_t left = 0;
+    void* get(size_t bytes);
+    void release();
+  } heap;
+  // Device work arrays of the lockstep solve: one block, kept from one call
+  // to the next and grown when a call needs more, so that a refinement's
+  // repeated solves and solve after solve allocate nothing. Freed with the
+  // plan, or at the end of a call when larger than kKeepBytes.
   struct SolveArena {
     static constexpr size_t kKeepBytes = size_t(16) << 30;
-    std::vector<void*> ptr;
-    std::vector<size_t> cap;
-    size_t next = 0;
-    void* get(size_t bytes);
-    void reset() { next = 0; }
-    size_t total() const;
+    char* base = nullptr;
+    size_t cap = 0, used = 0;
+    void reserve(size_t bytes);  // at least bytes in one block; carving restarts
+    void* get(size_t bytes);     // the next 256-byte aligned piece of the reservation
     void release();
   } arena;
 
@@ -269,11 +279,8 @@ struct Plan {
                  std::vector<double2>& h2all) const;
   template <class T>
   T* alloc(size_t count) {
-    void* p = nullptr;
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-    if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    allocations.push_back(p);
+    void* p = heap.get(count * sizeof(T));
     bytes += count * sizeof(T);
     return static_cast<T*>(p);
   }
@@ -352,9 +359,13 @@ struct Store<float2> {
 
 // Device work (setup_kernels.cu / matvec_kernels.cu)
 void launch_patterns(Plan& P, int medium, cudaStream_t s);
+// Transfer factors of one (medium, level) into out. The kernel's inputs go
+// to the device in one block: from the plan's heap while the plan is built
+// (in_heap), else a temporary allocation.
 void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& rhat,
                      const std::vector<int>& hoff, const std::vector<int>& hL,
-                     const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s);
+                     const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s,
+                     bool in_heap = false);
 void launch_near(Plan& P, cudaStream_t s);
 // Z[3 pos[i] + 1] = z12[i] for n entries of the near field (device arrays).
 void launch_near_z12_scatter(double2* Z, const long long* pos, const double2* z12, long long n, cudaStream_t s);
@@ -363,7 +374,12 @@ void clear_graphs(Plan& P);  // after any change that alters what an apply launc
 // Batched apply: W[j] = A X[j] for j < R; X[j] at X + j * ldx (ldx >= 2N),
 // the same for W. Right-hand sides go through in groups of kBatchSlots.
 constexpr int kBatchSlots = 16;
-void reserve_batch(Plan& P, int R);  // allocates the leaf-level arrays of min(R, kBatchSlots) slots
+// Allocates the complex64 slot tree (mixed plans) and, with fp64, the FP64
+// leaf-level arrays of min(R, kBatchSlots) slots.
+void reserve_batch(Plan& P, int R, bool fp64);
+// Allocates d_xb / d_wb (kBatchSlots vectors each), the staging of
+// host-pointer batched applies and of the refinement's FP64 residuals.
+void reserve_batch_staging(Plan& P);
 void apply_batch_device(Plan& P, int R, const double2* X, long long ldx, double2* W, long long ldw, cudaStream_t s);
 // The complex64 operator (precision = mixed plans): complex128 x and w, every
 // table and workspace in complex64, FP32 arithmetic. Fixed kernel choices:

@@ -456,19 +456,31 @@ void launch_patterns(Plan& P, int medium, cudaStream_t s) {
 
 void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& rhat,
                      const std::vector<int>& hoff, const std::vector<int>& hL,
-                     const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s) {
+                     const std::vector<double2>& h2, bool weighted, double2* out, cudaStream_t s, bool in_heap) {
   const MediumLevel& M = P.ml[medium][level];
   const int nvec = static_cast<int>(hL.size());
   if (nvec == 0) return;
-  double* d_rhat = nullptr;
-  int *d_hoff = nullptr, *d_hL = nullptr;
-  double2* d_h2 = nullptr;
-  double* d_wth = nullptr;
-  MLFMA_CUDA(cudaMalloc(&d_rhat, rhat.size() * sizeof(double)));
-  MLFMA_CUDA(cudaMalloc(&d_hoff, hoff.size() * sizeof(int)));
-  MLFMA_CUDA(cudaMalloc(&d_hL, hL.size() * sizeof(int)));
-  MLFMA_CUDA(cudaMalloc(&d_h2, h2.size() * sizeof(double2)));
-  MLFMA_CUDA(cudaMalloc(&d_wth, M.grid.wth.size() * sizeof(double)));
+  // one device block for the five inputs, each part 256-byte aligned
+  auto part = [](size_t bytes) { return (bytes + 255) & ~size_t(255); };
+  const size_t b_rhat = part(rhat.size() * sizeof(double)), b_hoff = part(hoff.size() * sizeof(int)),
+               b_hL = part(hL.size() * sizeof(int)), b_h2 = part(h2.size() * sizeof(double2));
+  const size_t total = b_rhat + b_hoff + b_hL + b_h2 + part(M.grid.wth.size() * sizeof(double));
+  char* blk = nullptr;
+  if (in_heap)
+    blk = P.alloc<char>(total);
+  else
+    MLFMA_CUDA(cudaMalloc(&blk, total));
+  struct Owned {
+    char* p;
+    ~Owned() {
+      if (p) cudaFree(p);
+    }
+  } owned{in_heap ? nullptr : blk};
+  double* d_rhat = reinterpret_cast<double*>(blk);
+  int* d_hoff = reinterpret_cast<int*>(blk + b_rhat);
+  int* d_hL = reinterpret_cast<int*>(blk + b_rhat + b_hoff);
+  double2* d_h2 = reinterpret_cast<double2*>(blk + b_rhat + b_hoff + b_hL);
+  double* d_wth = reinterpret_cast<double*>(blk + b_rhat + b_hoff + b_hL + b_h2);
   MLFMA_CUDA(cudaMemcpyAsync(d_rhat, rhat.data(), rhat.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   MLFMA_CUDA(cudaMemcpyAsync(d_hoff, hoff.data(), hoff.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   MLFMA_CUDA(cudaMemcpyAsync(d_hL, hL.data(), hL.size() * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -480,11 +492,6 @@ void launch_transfer(Plan& P, int medium, int level, const std::vector<double>& 
                                          M.K, nvec, weighted ? 1 : 0, out);
   MLFMA_CUDA(cudaGetLastError());
   MLFMA_CUDA(cudaStreamSynchronize(s));
-  cudaFree(d_rhat);
-  cudaFree(d_hoff);
-  cudaFree(d_hL);
-  cudaFree(d_h2);
-  cudaFree(d_wth);
 }
 
 __global__ void near_z12_scatter_kernel(double2* __restrict__ Z, const long long* __restrict__ pos,

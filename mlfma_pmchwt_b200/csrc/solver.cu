@@ -463,14 +463,12 @@ void rhs_pmchwt(Plan& P, const double kinc[3], const double einc[3], const doubl
     a.einc[c] = einc[c];
     a.hinc[c] = hinc[c];
   }
-  double2* d = nullptr;
-  MLFMA_CUDA(cudaMalloc(&d, 2 * static_cast<size_t>(P.N) * sizeof(double2)));
-  rhs_kernel<<<(P.N + 127) / 128, 128, 0, P.stream>>>(a, d);
-  cudaError_t e = cudaMemcpyAsync(V, d, 2 * static_cast<size_t>(P.N) * sizeof(double2), cudaMemcpyDeviceToHost,
-                                  P.stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(P.stream);
-  cudaFree(d);
-  MLFMA_CUDA(e);
+  // into the plan's staging vector for host-pointer applies (one call in flight per plan)
+  rhs_kernel<<<(P.N + 127) / 128, 128, 0, P.stream>>>(a, P.d_w);
+  MLFMA_CUDA(cudaGetLastError());
+  MLFMA_CUDA(cudaMemcpyAsync(V, P.d_w, 2 * static_cast<size_t>(P.N) * sizeof(double2), cudaMemcpyDeviceToHost,
+                             P.stream));
+  MLFMA_CUDA(cudaStreamSynchronize(P.stream));
 }
 
 void rcs_pmchwt(Plan& P, const double* I, int n_angles, const double* theta_deg, const double* phi_deg,
