@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(128, 1) agg_tc_kernel(const __grid_constant__ 
     }
     // one verdict for the whole CTA: the TMEM loads below are warp-collective
     // and the loop's barriers must be reached by every thread
-    ok = __syncthreads_and(mbar_wait(bar, phase, a.status, false)) != 0;
+    ok = __syncthreads_and(mbar_wait(bar, phase, a.status, false, kStatusAggTc)) != 0;
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
       uint32_t* const Bh = Ah + 2 * kLfStageA;
       uint32_t* const Bl = Bh + kLfStageB;
       if (gc >= 2)  // the stage's previous MMAs (chunk gc - 2) are done
-        ok = __syncthreads_and(mbar_wait(bar + st, ((gc - 2) >> 1) & 1, a.status, false)) != 0;
+        ok = __syncthreads_and(mbar_wait(bar + st, ((gc - 2) >> 1) & 1, a.status, false, kStatusLeafTc)) !=
+             0;
       if (!ok) break;
       if (c >= 2) {  // chunk c - 2 of this medium is in the stage's accumulator
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -382,7 +383,8 @@ __global__ void __launch_bounds__(128, 1) leaf_tc_kernel(const __grid_constant__
     }
     if (!ok) break;
     // the medium's last (up to) two chunks: their accumulators
-    ok = __syncthreads_and(mbar_wait(bar + ((gc - 1) & 1), ((gc - 1) >> 1) & 1, a.status, false)) != 0;
+    ok = __syncthreads_and(
+             mbar_wait(bar + ((gc - 1) & 1), ((gc - 1) >> 1) & 1, a.status, false, kStatusLeafTc)) != 0;
     if (!ok) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (nchunk >= 2) drain((gc - 2) & 1);

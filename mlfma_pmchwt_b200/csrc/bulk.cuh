@@ -11,6 +11,8 @@ namespace mlfma {
 
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
 constexpr int kStatusWaitTimeout = 1;
+// which kernel's wait ran out (or'ed with kStatusWaitTimeout)
+constexpr int kStatusAggTc = 2, kStatusLeafTc = 4, kStatusM2lGrp = 8;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -60,8 +62,9 @@ __device__ __forceinline__ int status_now(const int* status) {
 // status bit set) when it has not after kWaitNs. With give_up, the wait also
 // ends early once another CTA has recorded a status bit, so that one failure
 // does not cost every CTA of the launch its full wait; a wait for copies
-// already issued passes give_up = false.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, bool give_up = true) {
+// already issued passes give_up = false. site: the kernel's status bit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, bool give_up = true,
+                                          int site = 0) {
   if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   for (;;) {
@@ -69,7 +72,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* s
       if (mbar_test(bar, parity)) return true;
     if (give_up && status_now(status) != 0) return false;
     if (global_ns() - t0 > kWaitNs) {
-      atomicOr(status, kStatusWaitTimeout);
+      atomicOr(status, kStatusWaitTimeout | site);
       return false;
     }
   }

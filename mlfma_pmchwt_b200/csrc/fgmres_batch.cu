@@ -406,6 +406,7 @@ void back_substitute(const std::vector<C>& H, int ld, const std::vector<C>& s, i
 
 // Host side of the batched vector steps on one stream, for up to R positions.
 struct BatchOps {
+  Plan& P;  // its device status is read at every host sync
   cudaStream_t s;
   long long n;
   int nblk;          // blocks per system
@@ -430,7 +431,9 @@ struct BatchOps {
     norms_dev(Ra, sys, w, b, r, has_b);
     hbuf.resize(static_cast<size_t>(Ra) * (2 * ldp + 2));
     MLFMA_CUDA(cudaMemcpyAsync(hbuf.data(), hdev, hbuf.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    fetch_device_status(P, s);
     MLFMA_CUDA(cudaStreamSynchronize(s));
+    raise_device_status(P);
     std::vector<double> out(Ra);
     for (int a = 0; a < Ra; ++a) out[a] = std::sqrt(hbuf[static_cast<size_t>(a) * (2 * ldp + 2)].real());
     return out;
@@ -454,7 +457,9 @@ struct BatchOps {
     orthogonalise_dev(Ra, sys, V, w, nv);
     hbuf.resize(static_cast<size_t>(Ra) * ldh);
     MLFMA_CUDA(cudaMemcpyAsync(hbuf.data(), hdev, hbuf.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    fetch_device_status(P, s);
     MLFMA_CUDA(cudaStreamSynchronize(s));
+    raise_device_status(P);
     hcol.assign(Ra, std::vector<C>(nv));
     hn.assign(Ra, 0.0);
     for (int a = 0; a < Ra; ++a) {
@@ -516,7 +521,7 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   double2* wk[kN];
   for (int i = 0; i < kN; ++i) wk[i] = cnt[i] ? static_cast<double2*>(P.arena.get(cnt[i] * sizeof(double2))) : nullptr;
   double2 *x = wk[kX], *b = wk[kB], *r = wk[kR], *V = wk[kV], *Zd = wk[kZ], *Q = wk[kQ], *Xs = wk[kXs], *Ws = wk[kWs];
-  BatchOps ops{s, n, nblk, ldp};
+  BatchOps ops{P, s, n, nblk, ldp};
   ops.part = wk[kPart];
   ops.hdev = wk[kH];
   ops.alpha = reinterpret_cast<double*>(wk[kAlpha]);
@@ -535,6 +540,7 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
     ib.beta = reinterpret_cast<double*>(wk[kIBeta]);
     ib.done = reinterpret_cast<int*>(wk[kIDone]);
   }
+  MLFMA_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int), s));
   MLFMA_CUDA(cudaMemcpyAsync(x, xh, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyHostToDevice, s));
   MLFMA_CUDA(cudaMemcpyAsync(b, rhs, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyHostToDevice, s));
   st.assign(R, SolveStats());
@@ -739,7 +745,9 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
     live = keep;
   }
   MLFMA_CUDA(cudaMemcpyAsync(xh, x, static_cast<size_t>(R) * n * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  fetch_device_status(P, s);
   MLFMA_CUDA(cudaStreamSynchronize(s));
+  raise_device_status(P);
   if (P.arena.cap > Plan::SolveArena::kKeepBytes) P.arena.release();
   seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   for (int q = 0; q < R; ++q) {

@@ -771,6 +771,9 @@ LearnedWork& lp_work(Plan& P) {
   w->S = P.alloc<float>(kLpH);
   w->w_scratch = P.alloc<__nv_bfloat16>(kLpParams);
   w->w_store = P.alloc<__nv_bfloat16>(kLpParams);
+  // the tables above are uploaded on the plan's stream; the learned kernels
+  // may run on a caller's stream
+  MLFMA_CUDA(cudaStreamSynchronize(P.stream));
   MLFMA_CUDA(cudaFuncSetAttribute(lp_layer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(layer_smem())));
   MLFMA_CUDA(cudaFuncSetAttribute(lp_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -866,7 +869,10 @@ void lp_attach(Plan& P, const float* params, int n) {
   LearnedWork& W = lp_work(P);
   std::vector<__nv_bfloat16> h(kLpParams);
   for (int i = 0; i < kLpParams; ++i) h[i] = __float2bfloat16_rn(params[i]);
-  MLFMA_CUDA(cudaMemcpy(W.w_store, h.data(), kLpParams * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+  // complete before the weights are used, on any stream
+  MLFMA_CUDA(cudaMemcpyAsync(W.w_store, h.data(), kLpParams * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice,
+                             P.stream));
+  MLFMA_CUDA(cudaStreamSynchronize(P.stream));
   W.w_attached = W.w_store;
 }
 

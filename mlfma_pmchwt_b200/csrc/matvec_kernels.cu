@@ -915,7 +915,8 @@ __global__ void __launch_bounds__(32 * (kGrpBoxes / kBW + 1)) m2l_grp_kernel(con
         const int4 cj = make_int4(__shfl_sync(0xffffffffu, cd.x, j), __shfl_sync(0xffffffffu, cd.y, j),
                                   __shfl_sync(0xffffffffu, cd.z, j), __shfl_sync(0xffffffffu, cd.w, j));
         const int st = i % kGrpStages;
-        const bool waited = i < kGrpStages || mbar_wait(empty + st, ((i / kGrpStages) - 1) & 1, a.status);
+        const bool waited =
+            i < kGrpStages || mbar_wait(empty + st, ((i / kGrpStages) - 1) & 1, a.status, true, kStatusM2lGrp);
         if (!__all_sync(0xffffffffu, waited)) {
           ok = false;
           break;
@@ -951,7 +952,7 @@ __global__ void __launch_bounds__(32 * (kGrpBoxes / kBW + 1)) m2l_grp_kernel(con
     // copy into its shared memory outstanding
     if (lane == 0)
       for (int q = max(0, i - kGrpStages); q < i; ++q)
-        mbar_wait(full + q % kGrpStages, (q / kGrpStages) & 1, a.status, false);
+        mbar_wait(full + q % kGrpStages, (q / kGrpStages) & 1, a.status, false, kStatusM2lGrp);
     return;
   }
 
@@ -964,7 +965,7 @@ __global__ void __launch_bounds__(32 * (kGrpBoxes / kBW + 1)) m2l_grp_kernel(con
   bool ok = true;
   for (int i = 0; i < n; ++i) {
     const int st = i % kGrpStages;
-    if (!mbar_wait(full + st, (i / kGrpStages) & 1, a.status)) {
+    if (!mbar_wait(full + st, (i / kGrpStages) & 1, a.status, true, kStatusM2lGrp)) {
       ok = false;
       break;
     }

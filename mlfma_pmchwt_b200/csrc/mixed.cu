@@ -48,7 +48,9 @@ std::vector<double> fp64_residuals(Plan& P, const std::vector<int>& list, const 
     for (int j = 0; j < rn; ++j) apply_device(P, Xd + j * n, Wd + j * n, P.stream);
     std::vector<C> w(static_cast<size_t>(rn) * n);
     MLFMA_CUDA(cudaMemcpyAsync(w.data(), Wd, w.size() * sizeof(double2), cudaMemcpyDeviceToHost, P.stream));
+    fetch_device_status(P, P.stream);
     MLFMA_CUDA(cudaStreamSynchronize(P.stream));
+    raise_device_status(P);
     for (int j = 0; j < rn; ++j) {
       const int q = list[g0 + j];
       for (long long i = 0; i < n; ++i) Rr[q * n + i] = B[q * n + i] - w[j * n + i];
@@ -94,6 +96,7 @@ bool mixed_solve(Plan& P, double* xh, const double* rhs, int itr_max, int mr, do
   if (refine_max < 0) throw std::invalid_argument("refine_max must be non-negative");
   const auto t0 = std::chrono::steady_clock::now();
   MLFMA_CUDA(cudaSetDevice(P.device));
+  MLFMA_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int), P.stream));
   const long long n = 2LL * P.N;
   C* x = reinterpret_cast<C*>(xh);
   const C* b = reinterpret_cast<const C*>(rhs);
@@ -137,6 +140,7 @@ std::vector<char> mixed_batch_solve(Plan& P, int R, double* xh, const double* rh
   if (refine_max < 0) throw std::invalid_argument("refine_max must be non-negative");
   const auto t0 = std::chrono::steady_clock::now();
   MLFMA_CUDA(cudaSetDevice(P.device));
+  MLFMA_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int), P.stream));
   reserve_batch(P, R, false);
   reserve_batch_staging(P);  // the FP64 residuals' device rows
   const long long n = 2LL * P.N;

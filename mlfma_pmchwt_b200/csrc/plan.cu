@@ -78,6 +78,22 @@ void Plan::SolveArena::release() {
   cap = used = 0;
 }
 
+void fetch_device_status(Plan& P, cudaStream_t s) {
+  check_cuda(cudaMemcpyAsync(P.h_status, P.d_status, sizeof(int), cudaMemcpyDeviceToHost, s), "status copy");
+}
+
+void raise_device_status(const Plan& P) {
+  const int v = *P.h_status;
+  if (v == 0) return;
+  std::string where;
+  if (v & 2) where += " tensor-core aggregation,";
+  if (v & 4) where += " tensor-core far-field testing,";
+  if (v & 8) where += " staged translation,";
+  if (!where.empty()) where.pop_back();
+  throw CudaError("device status " + std::to_string(v) + ": a bounded wait ran out in" +
+                  (where.empty() ? std::string(" a kernel") : where));
+}
+
 Plan::~Plan() {
   if (device >= 0) {
     cudaSetDevice(device);

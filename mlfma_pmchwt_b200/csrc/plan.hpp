@@ -261,6 +261,7 @@ struct Plan {
     void* get(size_t bytes);
     void release();
   } heap;
+  std::vector<std::pair<void*, size_t>> arrays;  // every array of the heap (address, bytes), in allocation order
   // Device work arrays of the lockstep solve: one block, kept from one call
   // to the next and grown when a call needs more, so that a refinement's
   // repeated solves and solve after solve allocate nothing. Freed with the
@@ -281,14 +282,21 @@ struct Plan {
   T* alloc(size_t count) {
     if (count == 0) count = 1;
     void* p = heap.get(count * sizeof(T));
+    arrays.emplace_back(p, count * sizeof(T));
     bytes += count * sizeof(T);
     return static_cast<T*>(p);
   }
+  // A device copy of v, ordered on the plan's stream: kernels on that stream
+  // see it; other streams only after a synchronisation of it. (A blocking
+  // cudaMemcpy from pageable memory may return before its DMA lands and is
+  // not ordered with the plan's non-blocking streams: a kernel launched right
+  // after it could read the array before the copy.) The host vector may go
+  // as soon as this returns: a pageable source is staged by the call.
   template <class T>
   T* upload(const std::vector<T>& v) {
     T* p = alloc<T>(v.size());
     if (!v.empty()) {
-      cudaError_t e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+      cudaError_t e = cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream);
       if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMemcpy: ") + cudaGetErrorString(e));
     }
     return p;
@@ -374,6 +382,13 @@ void clear_graphs(Plan& P);  // after any change that alters what an apply launc
 // Batched apply: W[j] = A X[j] for j < R; X[j] at X + j * ldx (ldx >= 2N),
 // the same for W. Right-hand sides go through in groups of kBatchSlots.
 constexpr int kBatchSlots = 16;
+// Copies the plan's device status bits to its pinned host word on stream s
+// (read after the caller's synchronisation of s) ...
+void fetch_device_status(Plan& P, cudaStream_t s);
+// ... and throws when one is set (a bounded wait in a kernel ran out: that
+// apply's result is incomplete), naming the kernels.
+void raise_device_status(const Plan& P);
+
 // Allocates the complex64 slot tree (mixed plans) and, with fp64, the FP64
 // leaf-level arrays of min(R, kBatchSlots) slots.
 void reserve_batch(Plan& P, int R, bool fp64);
