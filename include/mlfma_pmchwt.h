@@ -199,6 +199,9 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  *                  and far-field testing on the CUDA cores; 1 = on the tensor
  *                  cores (tcgen05 kind::tf32 with high/low operand splitting,
  *                  boxes of at most 64 RWGs; default).
+ *   "batch_tree.variant" (the batched complex64 apply only) 0 = the tree
+ *                  passes of each right-hand side in turn; 1 = every level
+ *                  once for all right-hand sides on slot-major arrays (default).
  *   "leaf.variant" 0 = the near-field rows inside the leaf testing kernel (default);
  *                  1 = the near-field product on its own stream from the start
  *                  of the apply (it needs only x), overlapping the tree
@@ -214,9 +217,10 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  * at their current values) over `applies` applies of the plan's own operator
  * (device vectors owned by the plan) and keeps the fastest; variant_ms (may be
  * NULL) receives the per-apply ms of every value, keys in that order
- * (23 entries: m2l 0-8, up 0-3, l2l 0-1, agg 0-1, leaf 0-1, batch_tc 0-1, graph 0-1).
- * "batch_tc.variant" acts on the batched complex64 apply only: autotune
- * leaves it as set and reports -1 for its entries. */
+ * (25 entries: m2l 0-8, up 0-3, l2l 0-1, agg 0-1, leaf 0-1, batch_tc 0-1,
+ * batch_tree 0-1, graph 0-1). "batch_tc.variant" and "batch_tree.variant"
+ * act on the batched complex64 apply only: autotune leaves them as set and
+ * reports -1 for their entries. */
 MLFMA_API int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value);
 MLFMA_API int mlfma_get_tuning(const mlfma_plan* plan, const char* key);
 MLFMA_API int mlfma_autotune(mlfma_plan* plan, int applies, double* variant_ms);
