@@ -264,16 +264,33 @@ template <class Z>
 __global__ void __launch_bounds__(128) near_batch_box_kernel(NearBatchArg<Z> a) {
   extern __shared__ __align__(16) unsigned char near_smem[];
   Z* xsm = reinterpret_cast<Z*>(near_smem);
+  __shared__ const double2* xbase[kNearBoxRB];
   const int b = blockIdx.x;
   const int p0 = blockIdx.y * kNearBoxRB, pn = min(kNearBoxRB, a.R - p0);
   const int s0 = a.near_sptr[b], ns = a.near_sptr[b + 1] - s0;
   const int r0 = a.leaf_ptr[b], nb = a.leaf_ptr[b + 1] - r0;
-  for (int i = threadIdx.x; i < pn * ns; i += blockDim.x) {
-    const int j = i / ns, q = i - j * ns;
-    const double2* xj = a.x.at(p0 + j, a.sys);
+  if (threadIdx.x < pn) xbase[threadIdx.x] = a.x.at(p0 + threadIdx.x, a.sys);
+  __syncthreads();
+  // one source per thread, the values of 4 systems in flight at once
+  constexpr int kStage = 4;
+  for (int q = threadIdx.x; q < ns; q += blockDim.x) {
     const int src = a.near_src[s0 + q];
-    xsm[(2 * j) * ns + q] = Cx<Z>::from(xj[src]);
-    xsm[(2 * j + 1) * ns + q] = Cx<Z>::from(xj[a.N + src]);
+#pragma unroll
+    for (int j0 = 0; j0 < kNearBoxRB; j0 += kStage) {
+      double2 vJ[kStage], vM[kStage];
+#pragma unroll
+      for (int j = 0; j < kStage; ++j)
+        if (j0 + j < pn) {
+          vJ[j] = xbase[j0 + j][src];
+          vM[j] = xbase[j0 + j][a.N + src];
+        }
+#pragma unroll
+      for (int j = 0; j < kStage; ++j)
+        if (j0 + j < pn) {
+          xsm[(2 * (j0 + j)) * ns + q] = Cx<Z>::from(vJ[j]);
+          xsm[(2 * (j0 + j) + 1) * ns + q] = Cx<Z>::from(vM[j]);
+        }
+    }
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
