@@ -294,23 +294,35 @@ __global__ void __launch_bounds__(128) near_batch_box_kernel(NearBatchArg<Z> a) 
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  for (int tl = threadIdx.x >> 5; tl < nb; tl += blockDim.x / 32) {
-    const int id = a.leaf_rwg[r0 + tl];
+  const int nw = blockDim.x / 32;
+  // each warp takes two target rows at a time (tl and tl + nw): every
+  // staged source value read from shared memory serves both rows, and the
+  // two rows' near-field loads are in flight together. Each row's sums are
+  // formed in the same order as with one row per pass.
+  for (int tl = threadIdx.x >> 5; tl < nb; tl += 2 * nw) {
+    const int tl2 = tl + nw;
+    const bool two = tl2 < nb;
     const Z* Zr = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(tl) * ns);
-    Z nJ[kNearBoxRB], nM[kNearBoxRB];
+    const Z* Zr2 = a.near_z + 3 * (a.near_zoff[b] + static_cast<long long>(two ? tl2 : tl) * ns);
+    Z nJ[kNearBoxRB], nM[kNearBoxRB], nJ2[kNearBoxRB], nM2[kNearBoxRB];
 #pragma unroll
-    for (int j = 0; j < kNearBoxRB; ++j) nJ[j] = nM[j] = Cx<Z>::zero();
+    for (int j = 0; j < kNearBoxRB; ++j) nJ[j] = nM[j] = nJ2[j] = nM2[j] = Cx<Z>::zero();
     for (int q = lane; q < ns; q += 32) {
       const Z z11 = Zr[3 * q], z12 = Zr[3 * q + 1], z22 = Zr[3 * q + 2];
+      const Z y11 = Zr2[3 * q], y12 = Zr2[3 * q + 1], y22 = Zr2[3 * q + 2];
 #pragma unroll
       for (int j = 0; j < kNearBoxRB; ++j) {
         if (j < pn) {
           const Z xJ = xsm[(2 * j) * ns + q], xM = xsm[(2 * j + 1) * ns + q];
           nJ[j] = cfma(z11, xJ, cfma(z12, xM, nJ[j]));
           nM[j] = cfma(z22, xM, csub(nM[j], cmul(z12, xJ)));
+          nJ2[j] = cfma(y11, xJ, cfma(y12, xM, nJ2[j]));
+          nM2[j] = cfma(y22, xM, csub(nM2[j], cmul(y12, xJ)));
         }
       }
     }
+    const int id = a.leaf_rwg[r0 + tl];
+    const int id2 = a.leaf_rwg[r0 + (two ? tl2 : tl)];
 #pragma unroll
     for (int j = 0; j < kNearBoxRB; ++j) {
 #pragma unroll
@@ -319,11 +331,19 @@ __global__ void __launch_bounds__(128) near_batch_box_kernel(NearBatchArg<Z> a) 
         nJ[j].y += __shfl_xor_sync(0xffffffffu, nJ[j].y, o);
         nM[j].x += __shfl_xor_sync(0xffffffffu, nM[j].x, o);
         nM[j].y += __shfl_xor_sync(0xffffffffu, nM[j].y, o);
+        nJ2[j].x += __shfl_xor_sync(0xffffffffu, nJ2[j].x, o);
+        nJ2[j].y += __shfl_xor_sync(0xffffffffu, nJ2[j].y, o);
+        nM2[j].x += __shfl_xor_sync(0xffffffffu, nM2[j].x, o);
+        nM2[j].y += __shfl_xor_sync(0xffffffffu, nM2[j].y, o);
       }
       if (lane == 0 && j < pn) {
         double2* w = a.w.at(p0 + j, a.sys);
         w[id] = Cx<Z>::to64(nJ[j]);
         w[a.N + id] = Cx<Z>::to64(nM[j]);
+        if (two) {
+          w[id2] = Cx<Z>::to64(nJ2[j]);
+          w[a.N + id2] = Cx<Z>::to64(nM2[j]);
+        }
       }
     }
   }
