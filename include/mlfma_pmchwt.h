@@ -185,11 +185,17 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  *                  arithmetic, 2 boxes per warp; 7 = as 6 with 4 boxes per
  *                  warp. 2-7 launch the leaf level and the other levels of a
  *                  medium as two launches.
+ *   "m2l.pair_warps" tile shape of the pair translation (m2l variant 4 and
+ *                  the complex64 paths): 0 = 2, 1 = 4 (default), 2 = 8 box
+ *                  pairs (warps) per CTA.
  *   "up.variant"   interpolation: 0 = 9-tap gather per parent direction and
  *                  component (default); 1 = separable phi-then-theta in bands of
  *                  theta rows through shared memory; 2 = one thread per
  *                  (parent, direction) for all 6 components; 3 = separable in
  *                  registers, a phi column of 4 parent theta rows per thread.
+ *   "up.threads"   tile shape of the 9-tap interpolation (up variant 0 and the
+ *                  complex64 paths): 0 = 64, 1 = 128 (default), 2 = 256
+ *                  parent directions (threads) per CTA.
  *   "l2l.variant"  anterpolation: 0 = transposed 9-tap gather per child
  *                  direction; 1 = separable transposed theta-then-phi (default).
  *   "agg.variant"  aggregation: 0 = one thread per (leaf box, direction), one
@@ -217,8 +223,8 @@ MLFMA_API int mlfma_profile_read(mlfma_plan* plan, double* stage_ms, int* applie
  * at their current values) over `applies` applies of the plan's own operator
  * (device vectors owned by the plan) and keeps the fastest; variant_ms (may be
  * NULL) receives the per-apply ms of every value, keys in that order
- * (25 entries: m2l 0-8, up 0-3, l2l 0-1, agg 0-1, leaf 0-1, batch_tc 0-1,
- * batch_tree 0-1, graph 0-1). "batch_tc.variant" and "batch_tree.variant"
+ * (31 entries: m2l 0-8, m2l.pair_warps 0-2, up 0-3, up.threads 0-2, l2l 0-1,
+ * agg 0-1, leaf 0-1, batch_tc 0-1, batch_tree 0-1, graph 0-1). "batch_tc.variant" and "batch_tree.variant"
  * act on the batched complex64 apply only: autotune leaves them as set and
  * reports -1 for their entries. */
 MLFMA_API int mlfma_set_tuning(mlfma_plan* plan, const char* key, int value);

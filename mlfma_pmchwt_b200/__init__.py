@@ -363,7 +363,7 @@ class MLFMM:
     def get_tuning(self, key: str) -> int:
         return self._check(self._lib.mlfma_get_tuning(self._h, key.encode()))
 
-    TUNING_KEYS = (("m2l.variant", 9), ("up.variant", 4), ("l2l.variant", 2), ("agg.variant", 2), ("leaf.variant", 2), ("batch_tc.variant", 2), ("batch_tree.variant", 2), ("apply.graph", 2))
+    TUNING_KEYS = (("m2l.variant", 9), ("m2l.pair_warps", 3), ("up.variant", 4), ("up.threads", 3), ("l2l.variant", 2), ("agg.variant", 2), ("leaf.variant", 2), ("batch_tc.variant", 2), ("batch_tree.variant", 2), ("apply.graph", 2))
 
     def autotune(self, applies: int = 3) -> dict:
         """Times the values of each tuning key on this plan (one key at a

@@ -289,7 +289,9 @@ struct TuningKey {
 };
 constexpr TuningKey kTuningKeys[] = {
     {"m2l.variant", &mlfma::Tuning::m2l_variant, 9},
+    {"m2l.pair_warps", &mlfma::Tuning::m2l_pair_warps, 3},
     {"up.variant", &mlfma::Tuning::up_variant, 4},
+    {"up.threads", &mlfma::Tuning::up_threads, 3},
     {"l2l.variant", &mlfma::Tuning::l2l_variant, 2},
     {"agg.variant", &mlfma::Tuning::agg_variant, 2},
     {"leaf.variant", &mlfma::Tuning::leaf_variant, 2},

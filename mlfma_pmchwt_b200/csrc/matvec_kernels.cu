@@ -148,8 +148,9 @@ struct UpArg {
 // register count low enough for the occupancy this gather needs.
 // kSlots: grid.z = 6 x slots with the slot offsets of the batched tree; the
 // single apply instantiates without them.
-template <class C, bool kSlots = false>
-__global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
+// kT: threads per CTA (a tile of kT parent directions of one box and component)
+template <class C, bool kSlots = false, int kT = kThreads>
+__global__ void __launch_bounds__(kT) up_kernel(UpArg<C> a) {
   using R = typename Cx<C>::real;
   const int kk = blockIdx.y * blockDim.x + threadIdx.x;
   const int b = blockIdx.x;
@@ -179,6 +180,18 @@ __global__ void __launch_bounds__(kThreads) up_kernel(UpArg<C> a) {
     acc = cfma(e, v, acc);
   }
   (kSlots ? a.Sp + slot * a.slot_p : a.Sp)[(static_cast<size_t>(b) * 6 + c) * a.Kp + kk] = acc;
+}
+
+// grid: (parent boxes, direction tiles of t, zdim = 6 components x slots)
+template <class C, bool kSlots>
+void launch_up(int t, int boxes, int K, int zdim, const UpArg<C>& a, cudaStream_t s) {
+  const dim3 g(boxes, (K + t - 1) / t, zdim);
+  if (t == 64)
+    up_kernel<C, kSlots, 64><<<g, 64, 0, s>>>(a);
+  else if (t == 256)
+    up_kernel<C, kSlots, 256><<<g, 256, 0, s>>>(a);
+  else
+    up_kernel<C, kSlots, 128><<<g, 128, 0, s>>>(a);
 }
 
 // Interpolation (m2m), one thread per (parent box, parent direction) for all
@@ -728,14 +741,15 @@ struct M2lPairArg {
 // kSlots: the slot offsets of the batched tree (grid.y = slot); the single
 // apply instantiates without them (two registers fewer: 96 rather than 98 in
 // FP64, which keeps five CTAs per SM).
-template <class C, bool kSlots = false>
-__global__ void __launch_bounds__(32 * kPairWarps) m2l_pair_kernel(const __grid_constant__ M2lPairArg<C> a) {
+// kW: box pairs (warps) per CTA.
+template <class C, bool kSlots = false, int kW = kPairWarps>
+__global__ void __launch_bounds__(32 * kW) m2l_pair_kernel(const __grid_constant__ M2lPairArg<C> a) {
   int si = 0;
   while (si + 1 < a.nseg && static_cast<int>(blockIdx.x) >= a.seg[si + 1].cta_begin) ++si;
   const M2lPairSeg<C>& g = a.seg[si];
   const int local = blockIdx.x - g.cta_begin;
   const int grp = local / g.nchunk;
-  const int pg = grp * kPairWarps + (threadIdx.x >> 5);
+  const int pg = grp * kW + (threadIdx.x >> 5);
   const int k = (local - grp * g.nchunk) * 32 + (threadIdx.x & 31);
   const int K = g.K;
   if (2 * pg >= g.B || k >= K) return;
@@ -819,6 +833,20 @@ __global__ void __launch_bounds__(64 * kPairWarps) m2l_pairh_kernel(const __grid
 #pragma unroll
     for (int c = 0; c < 3; ++c) out1[static_cast<size_t>(c) * K] = a1[c];
   }
+}
+
+// Tile shapes chosen at run time (tuning keys "m2l.pair_warps", "up.threads").
+inline int pair_warps(const Plan& P) { return 2 << P.tuning.m2l_pair_warps; }
+inline int up_threads(const Plan& P) { return 64 << P.tuning.up_threads; }
+
+template <class C, bool kSlots>
+void launch_m2l_pair(int w, dim3 grid, const M2lPairArg<C>& a, cudaStream_t st) {
+  if (w == 2)
+    m2l_pair_kernel<C, kSlots, 2><<<grid, 64, 0, st>>>(a);
+  else if (w == 8)
+    m2l_pair_kernel<C, kSlots, 8><<<grid, 256, 0, st>>>(a);
+  else
+    m2l_pair_kernel<C, kSlots, 4><<<grid, 128, 0, st>>>(a);
 }
 
 // Translation with staged sources: a CTA takes a group of 8 Morton-
@@ -1466,8 +1494,7 @@ void launch_up(Plan& P, int m, const LeafView& v, cudaStream_t s) {
     } else {
       UpArg<double2> a{Sc, pm.S, P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
                        pm.ph_up, pm.K, pm.nph, cm.K, cm.nph};
-      dim3 gu(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6);
-      up_kernel<double2><<<gu, kThreads, 0, s>>>(a);
+      launch_up<double2, false>(up_threads(P), P.lv[l].B, pm.K, 6, a, s);
     }
   }
 }
@@ -1496,12 +1523,13 @@ void launch_m2l(Plan& P, int m, const LeafView& v, cudaStream_t s, int lo, int h
       g = M2lPairSeg<double2>{level_S(P, m, l, v), level_B(P, m, l, v), cm.tfw, P.lv[l].pair_ptr, P.lv[l].pair_src,
                               P.lv[l].pair_vec,    P.lv[l].B,           cm.K,   (cm.K + 31) / 32,  ctas};
       const int G = (P.lv[l].B + 1) / 2;
-      ctas += ((G + kPairWarps - 1) / kPairWarps) * g.nchunk;
+      const int w = P.tuning.m2l_variant == 5 ? kPairWarps : pair_warps(P);
+      ctas += ((G + w - 1) / w) * g.nchunk;
     }
     if (P.tuning.m2l_variant == 5)
       m2l_pairh_kernel<double2><<<ctas, 64 * kPairWarps, 0, s>>>(a);
     else
-      m2l_pair_kernel<double2><<<ctas, 32 * kPairWarps, 0, s>>>(a);
+      launch_m2l_pair<double2, false>(pair_warps(P), dim3(ctas), a, s);
     return;
   }
   if (P.tuning.m2l_variant == 3) {
@@ -1674,9 +1702,9 @@ void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s, cudaStr
       M2lPairSeg<C>& g = t.seg[t.nseg++];
       g = M2lPairSeg<C>{S_at(l),          B_at(l),   Store<C>::tfw(cm), P.lv[l].pair_ptr, P.lv[l].pair_src,
                         P.lv[l].pair_vec, P.lv[l].B, cm.K,              (cm.K + 31) / 32, ctas};
-      ctas += (((P.lv[l].B + 1) / 2 + kPairWarps - 1) / kPairWarps) * g.nchunk;
+      ctas += (((P.lv[l].B + 1) / 2 + pair_warps(P) - 1) / pair_warps(P)) * g.nchunk;
     }
-    m2l_pair_kernel<C><<<ctas, 32 * kPairWarps, 0, st>>>(t);
+    launch_m2l_pair<C, false>(pair_warps(P), dim3(ctas), t, st);
   };
   if (sx) {
     MLFMA_CUDA(cudaEventRecord(ev_agg, s));
@@ -1689,7 +1717,7 @@ void tree_pass_fixed(Plan& P, int m, C* leafS, C* leafB, cudaStream_t s, cudaStr
     const MediumLevel& cm = P.ml[m][l + 1];
     UpArg<C> a{S_at(l + 1), S_at(l), P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx, pm.lp,
                Store<C>::ph_up(pm), pm.K, pm.nph, cm.K, cm.nph};
-    up_kernel<C><<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6), kThreads, 0, s>>>(a);
+    launch_up<C, false>(up_threads(P), P.lv[l].B, pm.K, 6, a, s);
   }
   if (sx) {
     translate(2, L - 1, s);
@@ -1729,9 +1757,9 @@ void tree_pass_slots(Plan& P, int m, int rn, cudaStream_t s, cudaStream_t sx, cu
       g = M2lPairSeg<C>{P.btS[m][l],      P.btB[m][l], cm.tfw32,          P.lv[l].pair_ptr, P.lv[l].pair_src,
                         P.lv[l].pair_vec, P.lv[l].B,   cm.K,              (cm.K + 31) / 32, ctas,
                         stride(l),        stride(l)};
-      ctas += (((P.lv[l].B + 1) / 2 + kPairWarps - 1) / kPairWarps) * g.nchunk;
+      ctas += (((P.lv[l].B + 1) / 2 + pair_warps(P) - 1) / pair_warps(P)) * g.nchunk;
     }
-    m2l_pair_kernel<C, true><<<dim3(ctas, rn), 32 * kPairWarps, 0, st>>>(t);
+    launch_m2l_pair<C, true>(pair_warps(P), dim3(ctas, rn), t, st);
     MLFMA_CUDA(cudaGetLastError());
   };
   MLFMA_CUDA(cudaEventRecord(ev_agg, s));
@@ -1744,7 +1772,7 @@ void tree_pass_slots(Plan& P, int m, int rn, cudaStream_t s, cudaStream_t sx, cu
     UpArg<C> a{P.btS[m][l + 1], P.btS[m][l], P.lv[l].child_begin, P.lv[l + 1].octant, pm.tidx, pm.lt, pm.pidx,
                pm.lp,           pm.ph_up32,  pm.K,                 pm.nph,              cm.K,    cm.nph,
                stride(l + 1),   stride(l)};
-    up_kernel<C, true><<<dim3(P.lv[l].B, (pm.K + kThreads - 1) / kThreads, 6 * rn), kThreads, 0, s>>>(a);
+    launch_up<C, true>(up_threads(P), P.lv[l].B, pm.K, 6 * rn, a, s);
   }
   translate(2, L - 1, s);
   MLFMA_CUDA(cudaStreamWaitEvent(s, ev_leaf, 0));

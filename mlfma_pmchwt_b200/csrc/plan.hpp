@@ -123,7 +123,11 @@ struct Tuning {
                                //    memory by bulk asynchronous copies, 2 boxes per warp;
                                // 7: as 6 with 4 boxes per warp; 8: as 7 with the source patterns
                                //    by TMA tile copies
+  int m2l_pair_warps = 1;      // box pairs (warps) per CTA of the pair translations (variants 4, 5 and the
+                               //    complex64 paths): 0 = 2, 1 = 4, 2 = 8
   int l2l_variant = 1;         // 0: 2-D transposed taps per child direction; 1: separable
+  int up_threads = 1;          // threads per CTA of the 9-tap interpolation (up variant 0 and the complex64
+                               //    paths): 0 = 64, 1 = 128, 2 = 256
   int up_variant = 0;          // 0: 9-tap gather per parent direction; 1: separable in bands;
                                // 2: 9-tap gather, all 6 components per thread;
                                // 3: separable in registers, 4-row bands per thread
