@@ -340,7 +340,7 @@ def solve_record(st: dict, inner_its: int) -> dict:
     return rec
 
 
-def multi_rhs_study(args, local: int) -> dict:
+def multi_rhs_study(args, local: int, mixed_only: bool = False) -> dict:
     """Many incidences on one body: sphere r = 2.5 lambda (icosphere sub 5,
     61,440 unknowns), eps_r 4, leaf 0.25 lambda; 128 plane waves, theta_i =
     i * 180/127, phi = 0, polarisation alternating theta / phi. Lockstep
@@ -369,6 +369,9 @@ def multi_rhs_study(args, local: int) -> dict:
     out["mixed_lockstep"] = record(sm, time.perf_counter() - t)
     out["mixed_lockstep"]["solver"] = ("lockstep FGMRES(50) with the complex64 operator and near-field "
                                        "preconditioner, FP64 refinement")
+    if mixed_only:
+        op.close()
+        return out
     t = time.perf_counter()
     Xd, sd = op.matrix_solver_batch(B, itr_max=500, mr=50, tol_abs=0.0, tol_rel=1e-3, inner_its=args.study_inner_its)
     out["fp64_lockstep"] = record(sd, time.perf_counter() - t)
@@ -665,6 +668,10 @@ def run_product(args):
         if rank == 0:
             print(json.dumps({"batched_apply": batched_apply_study(args, local, wl)}))
         return 0
+    if args.lockstep_only:  # the multi-RHS study's lockstep mixed solve alone (for profiler captures)
+        if rank == 0:
+            print(json.dumps({"multi_rhs": multi_rhs_study(args, local, mixed_only=True)}))
+        return 0
     if args.full_rhs_only:  # the 128-incidence study on the 245,760-unknown sphere alone
         if rank == 0:
             print(json.dumps({"multi_rhs_full": full_rhs_study(args, local)}))
@@ -905,6 +912,8 @@ def main(argv=None):
     ap.add_argument("--no-full-rhs", dest="full_rhs", action="store_false",
                     help="skip the 128-incidence study on the 245,760-unknown sphere (run with --size full)")
     ap.add_argument("--full-rhs-only", action="store_true", help="run only that study")
+    ap.add_argument("--lockstep-only", action="store_true",
+                    help="run only the multi-RHS study's lockstep mixed solve (61,440 unknowns, --rhs incidences)")
     ap.add_argument("--learned", action="store_true", help="also run the learned-preconditioner study")
     ap.add_argument("--learned-only", action="store_true", help="run only the learned-preconditioner study")
     ap.add_argument("--learned-bodies", type=int, default=24,
