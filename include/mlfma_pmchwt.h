@@ -136,9 +136,12 @@ MLFMA_API int mlfma_apply(mlfma_plan* plan, int n, const double* x, double* w);
 MLFMA_API int mlfma_apply_device(mlfma_plan* plan, int n, const void* x_dev, void* w_dev, void* stream);
 
 /* Device status bits of a plan after the device-pointer calls: synchronizes
- * the device and writes 0, or 1 when a bounded wait of the staged
- * translation (m2l.variant 6, 7) ran out and its output is not valid. The
- * host-pointer calls check the same bits and fail with MLFMA_ERR_CUDA. */
+ * the device and writes 0, or bit 1 when a bounded wait in a kernel ran out
+ * and the output of that call is not valid, with the kernel's bit beside it:
+ * 2 tensor-core aggregation, 4 tensor-core far-field testing, 8 staged
+ * translation (m2l.variant 6-8). The host-pointer calls and every host
+ * synchronisation of the solvers check the same bits and fail with
+ * MLFMA_ERR_CUDA (the solvers clear them when they start). */
 MLFMA_API int mlfma_device_status(mlfma_plan* plan, int* status);
 
 /* Batched apply: w[j] = A x[j] for R right-hand sides stored one after the
