@@ -65,13 +65,11 @@ mlfma::PlanParams to_params(const mlfma_params* p) {
 bool device_plan(const mlfma_plan* plan) { return plan && plan->p && plan->p->device >= 0; }
 
 // Waits for the plan's stream and raises if a kernel recorded a device
-// status bit (a bounded wait of the staged translation that ran out).
+// status bit (a bounded wait that ran out), naming the kernel.
 void sync_and_check(mlfma::Plan& P) {
-  MLFMA_CUDA(cudaMemcpyAsync(P.h_status, P.d_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+  mlfma::fetch_device_status(P, P.stream);
   MLFMA_CUDA(cudaStreamSynchronize(P.stream));
-  if (*P.h_status != 0)
-    throw mlfma::CudaError("device status " + std::to_string(*P.h_status) +
-                           ": a bounded wait in the staged translation ran out");
+  mlfma::raise_device_status(P);
 }
 
 }  // namespace
