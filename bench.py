@@ -65,7 +65,9 @@ def workload(args):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 25 ms; each sample is
+    stamped with the host clock when it arrives, and stop() keeps the samples
+    inside the window mark_begin() .. mark_end() (the timed region)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -74,34 +76,49 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
+        self.window = (None, None)
 
-    def start(self):
+    def start(self, wait_s: float = 3.0):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "25"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except (FileNotFoundError, OSError):
             self.proc = None
+            return
+        t = time.perf_counter()  # until the sampler is running
+        while not self.lines and time.perf_counter() - t < wait_s:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark_begin(self):
+        self.window = (time.perf_counter(), None)
+
+    def mark_end(self):
+        self.window = (self.window[0], time.perf_counter())
 
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.05)  # the sample that closes the window
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self._t.join(timeout=2)
+        t0, t1 = self.window
+        inside = [ln for t, ln in self.lines if t0 is not None and t1 is not None and t0 <= t <= t1 + 0.05]
+        rows = inside if inside else [ln for _, ln in self.lines]
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in rows:
             p = [q.strip() for q in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -114,7 +131,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "in_timed_region": bool(inside)}
 
 
 def dist_setup(backend: str = "nccl"):
@@ -712,15 +729,16 @@ def run_product(args):
     # timed region: device time, max over ranks
     clocks = ClockSampler(local)
     clocks.start()
-    time.sleep(0.4)
     barrier(world)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark_begin()
     e0.record(stream)
     for _ in range(args.steps):
         step()
     e1.record(stream)
     torch.cuda.synchronize(dev)
+    clocks.mark_end()
     barrier(world)
     clk = clocks.stop()
     ms_local = e0.elapsed_time(e1)
