@@ -81,6 +81,24 @@ def test_lockstep_solve_matches_single_solves(case_files, inner):
         assert st[0]["near_products"] == inner * st[0]["iterations"]
 
 
+def test_lockstep_work_arrays_kept_between_calls(case_files):
+    """The lockstep solve keeps its work arrays in the plan from one call to
+    the next (one block, grown when a call needs more): solves of 3, then 20,
+    then 2 systems on one plan give what fresh plans give, bit for bit."""
+    from mlfma_pmchwt_b200 import MLFMM
+    m, p, eps, leaf = case_files["sphere_s2"]
+    op = MLFMM(m, freq=FREQ, eps_r=eps, leaf_coeff=leaf, device=0)
+    B = _incidences(op, 20)
+    for rows in (slice(0, 3), slice(0, 20), slice(5, 7)):
+        X, st = op.matrix_solver_batch(B[rows], itr_max=300, mr=30, tol_rel=1e-5, inner_its=4)
+        fresh = MLFMM(m, freq=FREQ, eps_r=eps, leaf_coeff=leaf, device=0)
+        Xf, sf = fresh.matrix_solver_batch(B[rows], itr_max=300, mr=30, tol_rel=1e-5, inner_its=4)
+        fresh.close()
+        assert np.array_equal(X, Xf), rows
+        assert [s["iterations"] for s in st] == [s["iterations"] for s in sf]
+    op.close()
+
+
 def test_lockstep_solve_more_systems_than_slots(case_files):
     """More right-hand sides than one batched apply takes (16): the applies
     go through in groups; every system converges to its own solution."""
