@@ -265,7 +265,6 @@ struct Plan {
     void* get(size_t bytes);
     void release();
   } heap;
-  std::vector<std::pair<void*, size_t>> arrays;  // every array of the heap (address, bytes), in allocation order
   // Device work arrays of the lockstep solve: one block, kept from one call
   // to the next and grown when a call needs more, so that a refinement's
   // repeated solves and solve after solve allocate nothing. Freed with the
@@ -286,7 +285,6 @@ struct Plan {
   T* alloc(size_t count) {
     if (count == 0) count = 1;
     void* p = heap.get(count * sizeof(T));
-    arrays.emplace_back(p, count * sizeof(T));
     bytes += count * sizeof(T);
     return static_cast<T*>(p);
   }
