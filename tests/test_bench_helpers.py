@@ -29,3 +29,38 @@ def test_translation_flops_of_the_full_workload():
     k2 = [17672, 5832, 2178, 882, 450]
     op = SimpleNamespace(max_level=6, info=SimpleNamespace(far_pairs=pairs, K_k1=k1, K_k2=k2))
     assert bench.translation_flops(op) == 22338003456.0
+
+
+class _DoneProcess:
+    def terminate(self):
+        pass
+
+    def wait(self, timeout=None):
+        return 0
+
+
+def _sampler_with(lines, window):
+    s = bench.ClockSampler(0)
+    s.proc = _DoneProcess()
+    s._t = SimpleNamespace(join=lambda timeout=None: None)
+    s.lines = lines
+    s.window = window
+    return s
+
+
+def test_clock_samples_are_kept_inside_the_timed_region():
+    # index, clocks.sm, clocks.max.sm, power, active, hw_slowdown, hw_thermal, sw_thermal, sw_power_cap
+    idle = "0, 1200, 1965, 150, 0x0, Not Active, Not Active, Not Active, Not Active"
+    busy = "0, 1965, 1965, 900, 0x4, Not Active, Not Active, Not Active, Active"
+    lines = [(0.0, idle), (1.0, busy), (1.1, busy), (1.2, busy), (3.0, idle)]
+    got = _sampler_with(lines, (0.9, 1.25)).stop()
+    assert got["samples"] == 3 and got["in_timed_region"]
+    assert got["sm_mhz"] == 1965.0 and got["sm_max_mhz"] == 1965.0
+    assert got["reasons"] == ["sw_power_cap"]
+
+
+def test_clock_samples_fall_back_to_all_when_none_is_inside():
+    idle = "0, 1200, 1965, 150, 0x0, Not Active, Not Active, Active, Not Active"
+    got = _sampler_with([(0.0, idle), (0.5, idle)], (2.0, 2.1)).stop()
+    assert got["samples"] == 2 and not got["in_timed_region"]
+    assert got["reasons"] == ["sw_thermal_slowdown"]
