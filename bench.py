@@ -937,7 +937,7 @@ def main(argv=None):
     ap.add_argument("--learned-bodies", type=int, default=24,
                     help="training ellipsoids of the learned-preconditioner study")
     ap.add_argument("--learned-epochs", type=int, default=10)
-    ap.add_argument("--bodies-workers", type=int, default=4,
+    ap.add_argument("--bodies-workers", type=int, default=6,
                     help="bodies solved at once by the uneven-body study (host threads, one plan each)")
     ap.add_argument("--tuning", default="auto",
                     help="'auto' (autotune) or fixed kernel variants, e.g. m2l.variant=2,up.variant=1")
