@@ -547,11 +547,16 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   const size_t Rz = static_cast<size_t>(R);
   // work arrays (counts of complex128 values), in one block of the plan's
   // arena: no allocation when the last call's block is large enough
-  enum { kX, kB, kR, kV, kZ, kQ, kXs, kWs, kPart, kH, kAlpha, kM, kY, kSys, kIH, kICs, kISn, kIG, kIBeta, kIDone, kN };
+  // the preconditioner's input and output rows (by lockstep position) when
+  // its launches are replayed as a CUDA graph
+  const bool pgraph_on = inner_its > 0 && P.tuning.graph == 1 && lp_attached(P) == nullptr;
+  enum { kX, kB, kR, kV, kZ, kQ, kXs, kWs, kPart, kH, kAlpha, kM, kY, kSys, kIH, kICs, kISn, kIG, kIBeta, kIDone,
+         kPv, kPz, kN };
   const size_t cnt[kN] = {Rz * n, Rz * n, Rz * n, Rz * vs, inner_its > 0 ? Rz * zs : 0, inner_its > 0 ? Rz * qs : 0,
                           static_cast<size_t>(G) * n, static_cast<size_t>(G) * n, Rz * nblk * ldp,
                           Rz * (2 * ldp + 2), Rz, Rz, Rz * blas1::kMaxBasis, Rz,
-                          inner_its > 0 ? Rz * ldi * inner_its : 0, Rz * inner_its, Rz * inner_its, Rz * ldi, Rz, Rz};
+                          inner_its > 0 ? Rz * ldi * inner_its : 0, Rz * inner_its, Rz * inner_its, Rz * ldi, Rz, Rz,
+                          pgraph_on ? Rz * n : 0, pgraph_on ? Rz * n : 0};
   size_t work_bytes = 0;
   for (size_t c : cnt) work_bytes += (c * sizeof(double2) + 255) & ~size_t(255);
   P.arena.reserve(work_bytes);
@@ -630,13 +635,13 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
   const int ldh = 2 * ldp + 2;
   // z_q = (inner_its GMRES steps on Z_near from zero) applied to v_q, q in
   // list: every step is launches only, the host waits for none of them
-  auto precondition = [&](const std::vector<int>& list, long long voff, long long zoff) {
-    const int Ra = static_cast<int>(list.size());
+  // the launches of one preconditioner application to the Ra positions'
+  // vectors vin, writing zout
+  auto precondition_launch = [&](int Ra, VecRef vin, VecRef zout) {
     const int pb = (Ra + 63) / 64;
-    set_sys(list);
-    ops.norms_dev(Ra, sysd, sysref(V, vs, voff));
+    ops.norms_dev(Ra, sysd, vin);
     inner_begin_b<<<pb, 64, 0, s>>>(Ra, ops.hdev, ldh, ib, ops.alpha, ops.mdev);
-    scale_b<<<ops.grid(Ra), kBT, 0, s>>>(sysref(V, vs, voff), sysref(Q, qs, 0), sysd, n, ops.alpha);
+    scale_b<<<ops.grid(Ra), kBT, 0, s>>>(vin, sysref(Q, qs, 0), sysd, n, ops.alpha);
     for (int j = 0; j < inner_its; ++j) {
       {  // the preconditioner's near field is the complex64 copy at either precision
         NearBatchArg<float2> na{P.d_leaf_rwg,  P.d_rwg_leafbox,      P.d_leaf_ptr,
@@ -651,19 +656,66 @@ std::vector<char> fgmres_batch_solve(Plan& P, int R, double* xh, const double* r
           near_batch_kernel<float2><<<ng, 128, 0, s>>>(na);
         }
       }
-      for (int q : list) st[q].near_products++;
       ops.orthogonalise_dev(Ra, sysd, sysref(Q, qs, 0), sysref(Q, qs, (j + 1) * n), j + 1);
       inner_step_b<<<pb, 64, 0, s>>>(Ra, j, ops.hdev, ldh, ldp, ib, ops.alpha, ops.mdev);
       scale_b<<<ops.grid(Ra), kBT, 0, s>>>(sysref(Q, qs, (j + 1) * n), sysref(Q, qs, (j + 1) * n), sysd, n,
                                            ops.alpha);
     }
     inner_end_b<<<pb, 64, 0, s>>>(Ra, ib, ops.mdev, ops.ydev, blas1::kMaxBasis);
-    combine_b<<<ops.grid(Ra), kBT, 0, s>>>(sysref(Q, qs, 0), sysref(Zd, zs, zoff), sysd, n, ops.mdev, ops.ydev,
-                                           blas1::kMaxBasis, 0);
+    combine_b<<<ops.grid(Ra), kBT, 0, s>>>(sysref(Q, qs, 0), zout, sysd, n, ops.mdev, ops.ydev, blas1::kMaxBasis,
+                                           0);
     MLFMA_CUDA(cudaGetLastError());
-    // a learned correction of each z, when a network is attached to the plan
-    if (const __nv_bfloat16* wl = lp_attached(P))
-      for (int q : list) lp_forward(P, wl, V + q * vs + voff, Zd + q * zs + zoff, Zd + q * zs + zoff, false, s);
+  };
+  // With apply.graph 1 (and no learned correction) the ~10 launches per inner
+  // step are captured once as a CUDA graph on fixed input / output rows (the
+  // basis vector copied in, z copied out) and replayed at every outer step;
+  // the graph is captured again only when the number of iterating systems
+  // changes (the system list itself is read from the device at replay).
+  cudaGraphExec_t pexec = nullptr;
+  int pexec_ra = 0;
+  struct GraphGuard {
+    cudaGraphExec_t& e;
+    ~GraphGuard() {
+      if (e) cudaGraphExecDestroy(e);
+    }
+  } pguard{pexec};
+  auto precondition = [&](const std::vector<int>& list, long long voff, long long zoff) {
+    const int Ra = static_cast<int>(list.size());
+    set_sys(list);
+    for (int q : list) st[q].near_products += inner_its;
+    if (!pgraph_on) {
+      precondition_launch(Ra, sysref(V, vs, voff), sysref(Zd, zs, zoff));
+      // a learned correction of each z, when a network is attached to the plan
+      if (const __nv_bfloat16* wl = lp_attached(P))
+        for (int q : list) lp_forward(P, wl, V + q * vs + voff, Zd + q * zs + zoff, Zd + q * zs + zoff, false, s);
+      return;
+    }
+    double2* Pv = wk[kPv];
+    double2* Pz = wk[kPz];
+    ops.copy(Ra, sysd, sysref(V, vs, voff), posref(Pv));
+    if (pexec != nullptr && pexec_ra != Ra) {
+      MLFMA_CUDA(cudaGraphExecDestroy(pexec));
+      pexec = nullptr;
+    }
+    if (pexec == nullptr) {
+      MLFMA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      try {
+        precondition_launch(Ra, posref(Pv), posref(Pz));
+      } catch (...) {
+        cudaGraph_t gr = nullptr;
+        cudaStreamEndCapture(s, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        throw;
+      }
+      cudaGraph_t gr = nullptr;
+      MLFMA_CUDA(cudaStreamEndCapture(s, &gr));
+      const cudaError_t e = cudaGraphInstantiate(&pexec, gr, 0);
+      cudaGraphDestroy(gr);
+      MLFMA_CUDA(e);
+      pexec_ra = Ra;
+    }
+    MLFMA_CUDA(cudaGraphLaunch(pexec, s));
+    ops.copy(Ra, sysd, posref(Pz), sysref(Zd, zs, zoff));
   };
 
   const double eps = 1e-16;
